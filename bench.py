@@ -1,0 +1,355 @@
+"""Benchmark of the strip list-mode TOF MLEM path on B200.
+
+Workload (the at-scale configuration): two 800 mm strips at y = +-400 mm,
+800 x 400 image of 1 mm pixels, sigma_z 5 mm, sigma_dl 25 mm, 2e8 seeded
+synthetic events from a 10-ellipse Shepp-like phantom (activities 0.1-2.0).
+A step is one full-set MLEM iteration over all events; the metric is
+Mevent*iter/s (events x iterations / device time).  Events stay resident in
+HBM (2.4 GB > L2), so no L2 flush is needed between iterations.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 (torchrun, one rank per GPU): each rank holds its own 2e8 events
+(seed + rank); after every iteration's backprojection the ranks all-reduce
+the binary64 accumulator over NCCL and apply the same update (weak scaling).
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "j-pet-mlem-old_b200"))
+
+METRIC = "Strip TOF-MLEM Mevent·iter/s on 1 B200 at ≤1e-4 rel-L2 vs FP64 oracle"
+UNIT = "Mevent*iter/s"
+GEOM = dict(radius=400.0, length=800.0, n_y=400, n_z=800, p=1.0, s_z=5.0, s_dl=25.0)
+PHANTOM = [
+    (-150, 60, 40, 25, 20, 2.0),
+    (150, -60, 50, 30, -30, 0.1),
+    (0, 100, 60, 20, 0, 1.5),
+    (0, -110, 70, 25, 10, 0.5),
+    (-250, -40, 30, 30, 0, 1.8),
+    (250, 50, 35, 20, 45, 0.3),
+    (80, 40, 20, 15, 0, 2.0),
+    (-80, -60, 25, 15, -15, 0.8),
+    (0, 0, 300, 150, 0, 1.0),
+    (0, 0, 360, 175, 0, 0.2),
+]
+SEED = 20260101
+
+
+def workload_config(n_events, e2e_iters):
+    return {
+        "workload": "strip MLEM, 800x400 image of 1 mm pixels, R=400 mm, L=800 mm, "
+                    "sigma_z=5 mm, sigma_dl=25 mm, 10-ellipse Shepp-like phantom",
+        "n_events": n_events,
+        "image": [GEOM["n_y"], GEOM["n_z"]],
+        "pixel_mm": GEOM["p"],
+        "mode": "cpu-compat (GaussianKernel, no sensitivity)",
+        "accumulation": "kahan per lane + binary64 across lanes and images",
+        "step": "one full-set MLEM iteration over all events",
+        "e2e_step": f"set_events from pinned host + {e2e_iters} iterations + image D2H",
+        "l2": "inputs (12 B/event, 2.4 GB) larger than the 126 MB L2; no flush",
+        "parallelism": "events sharded per rank, image replicated",
+        "seed": SEED,
+    }
+
+
+def scanner():
+    import stripmlem as sm
+    return sm.Scanner(GEOM["radius"], GEOM["length"], GEOM["n_y"], GEOM["n_z"],
+                      GEOM["p"], GEOM["p"], GEOM["s_z"], GEOM["s_dl"])
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# reference arm / cpu baseline: the reference's own CPU binary
+# ---------------------------------------------------------------------------
+def run_reference_cpu(n_sample, iters, warmup, cores, events=None):
+    """Times the reference 2d_strip_reconstruction (oracle/_ref, built from the
+    reference sources with its default flags) on the first n_sample events of
+    the workload.  Returns (Mevent*iter/s, kind, detail)."""
+    from oracle import oracle as orc
+    import stripmlem as sm
+    sc = scanner()
+    if events is None:
+        zu, zd, dl = sm.generate_events(sc, PHANTOM, n_sample, seed=SEED)
+    else:
+        zu, zd, dl = (a[:n_sample] for a in events)
+    g = orc.geometry(GEOM["radius"], GEOM["length"], GEOM["n_y"], GEOM["n_z"],
+                     GEOM["p"], GEOM["p"], GEOM["s_z"], GEOM["s_dl"])
+    if orc.ref_available(nocontract=False):
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "events.bin")
+            orc.write_events_bin(path, zu, zd, dl)
+            _, out = orc.ref_benchmark(g, path, iters + warmup, cores)
+        times = [float(m.group(2)) for m in
+                 re.finditer(r"^\s*(\d+)\s+([0-9.]+)\s*$", out, flags=re.M)]
+        times = times[warmup:] if len(times) > warmup else times
+        t = sum(times) / 1000.0
+        return n_sample * len(times) / t / 1e6, "reference", \
+            f"first {n_sample} events of the workload, {len(times)} timed iterations " \
+            f"(+{warmup} warm-up) of oracle/_ref/2d_strip_reconstruction -T {cores} -vv"
+    # oracle port (single thread) when the reference binary was not built
+    t0 = time.perf_counter()
+    n = min(n_sample, 20000)
+    orc.mlem_f32(g, zu[:n], zd[:n], dl[:n], iters)
+    t = time.perf_counter() - t0
+    return n * iters / t / 1e6, "port", \
+        f"first {n} events, {iters} iterations of the oracle's binary32 restatement, 1 thread"
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    cores = host_cores()
+    n_sample = args.ref_events or min(args.events, 60000 * cores)
+    value, kind, sample = run_reference_cpu(n_sample, args.steps, args.warmup, cores)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": n_sample / (value * 1e6) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(args.events, args.e2e_iters),
+        "cpu_baseline": {"value": value, "unit": UNIT,
+                         "cores": cores if kind == "reference" else 1,
+                         "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def pinned_empty(n):
+    import torch
+    t = torch.empty(n, dtype=torch.float32, pin_memory=True)
+    return t, t.numpy()
+
+
+def ours(args, rank, world, local_rank):
+    import torch
+    import stripmlem as sm
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local_rank)
+    sc = scanner()
+    n = args.events
+
+    # seeded workload in pinned host memory (rank r: seed + r)
+    tz, zu = pinned_empty(n)
+    td, zd = pinned_empty(n)
+    tl, dl = pinned_empty(n)
+    from stripmlem import _lib
+    import ctypes
+    g = sc.geometry()
+    ph = (_lib.Ellipse * len(PHANTOM))(*[_lib.Ellipse(*map(float, e)) for e in PHANTOM])
+    rc = _lib.load().strip_generate_events(
+        ctypes.byref(g), ph, len(PHANTOM), SEED + rank, n,
+        zu.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+        zd.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+        dl.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+    assert rc == 0, rc
+
+    rec = sm.Reconstruction(sc, device=local_rank, mode=sm.MODE_CPU,
+                            accumulation=sm.ACCUM_KAHAN)
+    rec.set_events(zu, zd, dl)
+    st = rec.stats()
+    work_bb, work_in, nonempty = [ctypes.c_int64() for _ in range(3)]
+    rec._check(rec.lib.strip_count_work(rec._ctx, ctypes.byref(work_bb),
+                                        ctypes.byref(work_in), ctypes.byref(nonempty)))
+    flops_per_iter = 10.0 * work_bb.value + 18.0 * work_in.value  # work model
+
+    peak = ctypes.c_double()
+    rec._check(rec.lib.strip_probe_fp32_peak(local_rank, ctypes.byref(peak)))
+
+    # warm-up, then K timed iterations in one call (device time on the
+    # library's stream, CUDA events on both sides, synchronised)
+    rec(None, args.warmup)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        rec(None, args.steps)
+        torch.cuda.synchronize()
+    st = rec.stats()
+    t_ms = st["last_iterate_ms"]
+    tile_ms = st["last_tile_ms"]
+    launches = st["kernel_launches"]
+    if dist is not None:
+        tt = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    value = world * n * args.steps / (t_ms / 1e3) / 1e6
+    clocks = clk.summary()
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        img = np.empty((GEOM["n_y"], GEOM["n_z"]), np.float32)
+        times = []
+        for s in range(args.e2e_steps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rec.set_events(zu, zd, dl)
+            rec.rho = np.ones_like(img)
+            rec(None, args.e2e_iters)
+            img[...] = rec.rho
+            torch.cuda.synchronize()
+            if s > 0:
+                times.append(time.perf_counter() - t0)
+        e2e_t = max(times) if dist is None else max(times)
+        e2e = {"value": world * n * args.e2e_iters / (sum(times) / len(times)) / 1e6,
+               "unit": UNIT, "h2d_bytes_per_step": int(3 * 4 * n),
+               "d2h_bytes_per_step": int(img.nbytes), "steps": len(times),
+               "iterations_per_step": args.e2e_iters}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = host_cores()
+        n_sample = min(n, args.ref_events or 60000 * cores)
+        v, kind, sample = run_reference_cpu(n_sample, 1, 0, cores, events=(zu, zd, dl))
+        cpu = {"value": v, "unit": UNIT, "cores": cores if kind == "reference" else 1,
+               "kind": kind, "sample": sample}
+
+    achieved = flops_per_iter / (tile_ms / args.steps / 1e3) / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": workload_config(n, args.e2e_iters),
+        "roofline": {
+            "bound": "fp32", "achieved": achieved, "peak": peak.value,
+            "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None,
+            "traffic": None,
+            "kernel": "k_tile (tile-window MLEM kernel)",
+            "work_model": "10 flops per bbox pixel + 18 per in-ellipse pixel",
+            "bbox_pixels_per_iter": work_bb.value, "ellipse_pixels_per_iter": work_in.value,
+            "tile_ms_per_step": tile_ms / args.steps,
+            "peak_source": "measured live: strip_probe_fp32_peak (FMA chains, this GPU)",
+        },
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "binning": {k: st[k] for k in ("n_tiles_z", "n_tiles_y", "tile_z", "tile_y",
+                                       "halo_z", "halo_y", "n_work_items", "n_overflow",
+                                       "n_empty", "smem_bytes", "last_setup_ms")},
+    }
+    if e2e is not None:
+        line["e2e"] = e2e
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    rec.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--events", type=int, default=200_000_000)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-iters", type=int, default=20)
+    ap.add_argument("--ref-events", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", args.gpus))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if world > 1 and "RANK" not in os.environ:
+        sys.exit("for --gpus N > 1 launch under torchrun (one rank per GPU)")
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+    return ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

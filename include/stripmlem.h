@@ -1,0 +1,224 @@
+/*
+ * stripmlem.h -- C ABI of the B200 (sm_100a) strip list-mode TOF MLEM library.
+ *
+ * Drop-in boundary for the 2D strip reconstruction path of
+ * JPETTomography/j-pet-mlem-old.  The reference has no FFI; its operator API is
+ *   (1) the C++ template Reconstruction<F, Kernel> with public members
+ *       scanner / rho / sensitivity / responses and operator()(progress,
+ *       n_iterations, n_iterations_so_far)   (src/2d/strip/reconstruction.h:42-154)
+ *   (2) the GPU entry point PET2D::Strip::GPU::Reconstruction::run<F>(scanner,
+ *       responses, n_responses, rho_io, n_blocks, n_iterations_in_block,
+ *       output_cb, progress_cb, device, cuda_blocks, cuda_threads,
+ *       device_name_cb)                      (src/2d/strip/cuda/reconstruction.h:32-44)
+ *   (3) the 2d_strip_reconstruction CLI      (src/2d/strip/reconstruction_cmd.cpp:105-301)
+ * Each entry point below names the piece it replaces.
+ *
+ * Conventions: every function returns STRIP_OK (0) or a negative STRIP_E*
+ * code and never throws or aborts; the message of the last failure on a
+ * context is strip_last_error().  The caller owns every host buffer.  One
+ * context per host thread; all device work of a context is ordered on the
+ * context's own CUDA stream, and every call returns after that work is done.
+ *
+ * Image layout everywhere: row-major binary32, n_y_pixels rows of
+ * n_z_pixels; row 0 is the top (y = +size_y/2), column 0 is z = -size_z/2
+ * (scanner.h:136-144, reconstruction.h:67-72).
+ */
+#ifndef STRIPMLEM_H
+#define STRIPMLEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STRIPMLEM_ABI_VERSION 1
+
+enum strip_status {
+  STRIP_OK = 0,
+  STRIP_E_INVALID = -1,    /* bad argument (null pointer, size, geometry)    */
+  STRIP_E_CUDA = -2,       /* a CUDA runtime call failed                      */
+  STRIP_E_NOMEM = -3,      /* device or host allocation failed                */
+  STRIP_E_STATE = -4,      /* call out of order (e.g. iterate before events)  */
+  STRIP_E_KERNEL = -5,     /* a kernel reported an error through its status word */
+  STRIP_E_NODEVICE = -6    /* no CUDA device / driver                          */
+};
+
+/* Reconstruction semantics.
+ * STRIP_MODE_CPU: the reference CPU path -- GaussianKernel, no sensitivity:
+ *   rho'_j = sum_e K_ej rho_j / sum_k K_ek rho_k   (reconstruction.h:220-298)
+ * STRIP_MODE_GPU: the reference --gpu path -- AnalyticKernel with the 5-point
+ *   pixel sensitivity in the denominator (warp_granularity.cuh:347-399):
+ *   rho'_j = sum_e K_ej rho_j / sum_k K_ek s_k rho_k
+ *   i.e. the sensitivity-normalised LM-MLEM update with P = K * s.
+ * Both use the CPU's rule for an all-zero denominator (contribution 0). */
+enum strip_mode { STRIP_MODE_CPU = 0, STRIP_MODE_GPU = 1 };
+
+/* Accumulation of the per-event normalisation sums D_e = sum_k P_ek rho_k.
+ * FP32: plain binary32 per-lane sums; KAHAN: compensated binary32 per-lane
+ * sums; FP64: binary64 per-lane sums.  The cross-lane reduction and the
+ * global image/likelihood reductions are binary64 in every mode. */
+enum strip_accum { STRIP_ACCUM_FP32 = 0, STRIP_ACCUM_KAHAN = 1, STRIP_ACCUM_FP64 = 2 };
+
+/* Scanner parameters, in the units of the event file (the CLI's millimetres).
+ * Replaces Scanner<F, S>'s constructor arguments (scanner.h:39-67, options.h:42-50);
+ * the library narrows them to binary32 / int16 exactly as Scanner<float, short>
+ * does, so pixel sets match the reference bit for bit. */
+typedef struct strip_geometry {
+  double radius;              /* R: half the distance between the strips   */
+  double scintillator_length; /* L                                         */
+  int32_t n_y_pixels;
+  int32_t n_z_pixels;
+  double pixel_height;
+  double pixel_width;
+  double sigma_z;             /* TOF sigma along z                         */
+  double sigma_dl;            /* TOF sigma of delta-l                       */
+  double center_y;
+  double center_z;
+} strip_geometry;
+
+typedef struct strip_ctx strip_ctx;
+
+/* Iteration progress; replaces the run()'s progress delegate
+ * (cuda/reconstruction.h:38-39).  `finished` is 0 before and 1 after an
+ * iteration.  Return non-zero to stop after the current iteration. */
+typedef int (*strip_progress_cb)(int completed, int finished, void* user);
+
+/* Statistics of the last set_events / iterate. */
+typedef struct strip_stats {
+  int64_t n_events;          /* events held by the context                    */
+  int64_t n_empty;           /* events whose clamped box is empty (skipped)   */
+  int64_t n_overflow;        /* events processed on the global-memory path   */
+  int32_t n_tiles_z, n_tiles_y, tile_z, tile_y, halo_z, halo_y;
+  int32_t n_work_items;      /* (tile, event chunk) items per full pass        */
+  int32_t n_subsets;         /* subsets of the current binning                */
+  int32_t max_box_w, max_box_h;
+  int32_t smem_bytes;        /* dynamic shared memory per CTA                 */
+  int32_t kernel_launches;   /* launches of the last strip_iterate             */
+  double last_iterate_ms;    /* device time of the last strip_iterate          */
+  double last_setup_ms;      /* device time of the last set_events binning     */
+  double last_tile_ms;       /* device time of the tile-kernel launches of the
+                                last strip_iterate (CUDA events on the stream) */
+} strip_stats;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Creates a context on `device`.  Replaces the device selection and
+ * per-run state of GPU::Reconstruction::run (cuda/reconstruction.cu:54-74).
+ * The image starts at 1 everywhere, as Reconstruction's rho (reconstruction.h:59). */
+int strip_ctx_create(const strip_geometry* geometry, int device, strip_ctx** out);
+int strip_ctx_destroy(strip_ctx* ctx);
+/* Copies the last error message (NUL-terminated, truncated to size). */
+int strip_last_error(const strip_ctx* ctx, char* buf, size_t size);
+/* Device name, as run()'s device_name delegate (cuda/reconstruction.cu:55-57). */
+int strip_device_name(const strip_ctx* ctx, char* buf, size_t size);
+int strip_set_accumulation(strip_ctx* ctx, int accum);
+int strip_get_stats(const strip_ctx* ctx, strip_stats* out);
+
+/* ---- events ------------------------------------------------------------- */
+
+/* Host SoA events: z_u, z_d, dl.  Replaces ResponsesSOA (cuda/gpu_events_soa.h:15-44)
+ * and Reconstruction::responses.  Copies to the device, sorts the events into
+ * image tiles (n_subsets OSEM subsets: event e goes to subset e % n_subsets)
+ * and keeps them resident. */
+int strip_set_events(strip_ctx* ctx, const float* z_u, const float* z_d,
+                     const float* dl, int64_t n, int n_subsets);
+/* Host AoS events: n triples (z_u, z_d, dl), the reference's Response<float>
+ * layout and binary event-file layout (response.h:13-20, reconstruction.h:156-167). */
+int strip_set_responses(strip_ctx* ctx, const float* zu_zd_dl, int64_t n,
+                        int n_subsets);
+/* Same as strip_set_events with device pointers (already resident in HBM). */
+int strip_set_events_device(strip_ctx* ctx, const float* d_z_u,
+                            const float* d_z_d, const float* d_dl, int64_t n,
+                            int n_subsets);
+
+/* ---- image -------------------------------------------------------------- */
+
+/* rho in / out (host, n_y * n_z floats); Reconstruction::rho / run()'s rho_io. */
+int strip_set_image(strip_ctx* ctx, const float* rho);
+int strip_get_image(strip_ctx* ctx, float* rho);
+/* Sensitivity image: five_point = 1 gives Scanner::pixel_sensitivity
+ * (scanner.h:174-185, the --gpu path's texture); 0 gives the centre value
+ * Scanner::sensitivity (the CPU Reconstruction::sensitivity, reconstruction.h:67-73). */
+int strip_get_sensitivity(strip_ctx* ctx, int five_point, float* out);
+
+/* ---- reconstruction ------------------------------------------------------ */
+
+/* Runs n_iter MLEM iterations (n_subsets == 1) or OSEM iterations (each
+ * visits every subset once; subset update rho_j <- n_subsets * rho_j *
+ * sum_{e in subset} P_ej / D_e).  Replaces Reconstruction::operator()
+ * (reconstruction.h:109-154) and the iteration loop of run()
+ * (cuda/reconstruction.cu:79-110).  n_subsets must equal the binning of
+ * set_events, or the events are re-binned first.  `first` numbers the
+ * progress callbacks (n_iterations_so_far). */
+int strip_iterate(strip_ctx* ctx, int n_iter, int mode, int n_subsets,
+                  int first, strip_progress_cb progress, void* user);
+
+/* ---- differentiable projections (pixel sets fixed by the geometry's sigmas) */
+
+/* y_e = sum_j P_ej rho_j for every event, in the caller's event order, with
+ * the kernel evaluated at (sigma_z, sigma_dl).  rho and y are host buffers. */
+int strip_forward(strip_ctx* ctx, const float* rho, double sigma_z,
+                  double sigma_dl, int mode, double* y);
+/* g_j = sum_e P_ej w_e (adjoint / backprojection), w in event order. */
+int strip_adjoint(strip_ctx* ctx, const double* w, double sigma_z,
+                  double sigma_dl, int mode, double* g);
+/* d/d(sigma_z, sigma_dl) of sum_e w_e y_e, STRIP_MODE_CPU kernel. */
+int strip_grad_sigma(strip_ctx* ctx, const float* rho, const double* w,
+                     double sigma_z, double sigma_dl, double* d_sigma_z,
+                     double* d_sigma_dl);
+
+/* ---- parity ----------------------------------------------------------- */
+
+/* For n host events (z_u, z_d, dl): bbox pixels tested, in-ellipse pixels and
+ * the order-free set digest sum_p mix64(index_p + 1) (mod 2^64), where
+ * mix64 is the splitmix64 finaliser -- computed on the device by the same
+ * enumeration code the reconstruction kernels run.  Any output may be NULL.
+ * Replaces the DEBUG pixel dump of bb_update (reconstruction.h:257-286). */
+int strip_debug_pixel_sets(strip_ctx* ctx, const float* z_u, const float* z_d,
+                           const float* dl, int64_t n, int32_t* n_bb,
+                           int32_t* n_in, uint64_t* digest);
+
+/* ---- diagnostics ---------------------------------------------------------- */
+
+/* Totals over the context's events of the bounding-box pixels tested and the
+ * in-ellipse pixels (kernel evaluations) of one full pass, and the number of
+ * events with a non-empty pixel set.  Replaces ReconstructionStats'
+ * n_pixels_processed / n_kernel_calls (reconstruction_stats.h:7-89,
+ * reconstruction.h:260,272), which the reference can only collect in a
+ * special build. */
+int strip_count_work(strip_ctx* ctx, int64_t* n_bb, int64_t* n_in,
+                     int64_t* n_nonempty);
+
+/* Measures the device's binary32 FMA throughput (TFLOP/s, FMA = 2 flops) with
+ * a register-resident FMA chain kernel: the denominator of the roofline
+ * fraction of the (FP32-bound) reconstruction kernels.  No counterpart in the
+ * reference. */
+int strip_probe_fp32_peak(int device, double* tflops);
+
+/* ---- synthetic input ----------------------------------------------------- */
+
+/* Ellipse phantom region (the reference's phantom-file line
+ * "ellipse x y a b angle intensity", phantom.h:137-181; x is z). */
+typedef struct strip_ellipse {
+  double z, y, a, b, angle_deg, activity;
+} strip_ellipse;
+
+/* Seeded host generator of list-mode events in the reference's event format.
+ * Emission points are uniform in the union of the ellipses, overlaps
+ * exclusive with the first-listed ellipse on top (phantom.h:193-204);
+ * tan(theta) is uniform in (-L/(2R), L/(2R)); an emission counts only if both
+ * hits land on the strips (|z_u|,|z_d| < L/2, scanner.h:196-214); hits are
+ * then smeared by N(0, sigma_z) on z_u, z_d and N(0, sigma_dl) on dl
+ * (scanner.h:257-267).  Counter-based (Philox-4x32-10), so event i depends
+ * only on (seed, i) and the result does not depend on the thread count. */
+int strip_generate_events(const strip_geometry* g, const strip_ellipse* ellipses,
+                          int n_ellipses, uint64_t seed, int64_t n,
+                          float* z_u, float* z_d, float* dl);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STRIPMLEM_H */

@@ -1,0 +1,829 @@
+// C ABI of the strip MLEM library (include/stripmlem.h): contexts, event
+// binning, the iteration driver and the projection entry points.  The host
+// side owns no arithmetic that decides pixel sets; it only narrows the
+// scanner parameters to binary32 exactly as Scanner<float, short> does
+// (src/2d/strip/scanner.h:39-67) -- this translation unit is compiled with
+// -ffp-contract=off so those few host operations round as the reference's.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "stripmlem.h"
+#include "strip_internal.h"
+
+using namespace stripmlem;
+
+struct strip_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  char devname[256] = {0};
+  int sm_count = 148;
+  int smem_optin = 227 * 1024;
+  strip_geometry g{};
+  ScannerF s{};
+  int accum = STRIP_ACCUM_KAHAN;
+  int64_t n_pix = 0;
+  float* d_rho = nullptr;
+  double* d_acc = nullptr;
+  float* d_sens5 = nullptr;
+  // binned events
+  int64_t n_events = 0;   // as given by the caller
+  int64_t n_binned = 0;   // events with a non-empty box
+  float* d_zu = nullptr;
+  float* d_zd = nullptr;
+  float* d_dl = nullptr;
+  int64_t* d_perm = nullptr;
+  int n_subsets = 0;
+  Tiling t{};
+  int max_w = 0, max_h = 0;
+  std::vector<WorkItem> items;
+  WorkItem* d_items = nullptr;
+  std::vector<int> sub_item_begin, sub_item_count;
+  std::vector<int64_t> sub_g_begin, sub_g_count;
+  int* d_status = nullptr;
+  std::vector<cudaEvent_t> tile_marks;
+  strip_stats stats{};
+  std::string err;
+};
+
+namespace {
+
+int fail(strip_ctx* c, int code, const char* fmt, ...) {
+  if (c) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    c->err = buf;
+  }
+  return code;
+}
+
+#define CK(call)                                                         \
+  do {                                                                   \
+    cudaError_t e_ = (call);                                             \
+    if (e_ != cudaSuccess)                                               \
+      return fail(ctx, e_ == cudaErrorMemoryAllocation ? STRIP_E_NOMEM   \
+                                                       : STRIP_E_CUDA,   \
+                  "%s: %s (%s:%d)", #call, cudaGetErrorString(e_),       \
+                  __FILE__, __LINE__);                                   \
+  } while (0)
+
+int16_t narrow16(int32_t v) { return (int16_t)(uint16_t)(uint32_t)v; }
+
+// Scanner<float, short>(R, L, n_y, n_z, p_h, p_w, s_z, s_dl, c_y, c_z) and
+// GaussianKernel<float>(s_z, s_dl): scanner.h:50-67, gaussian_kernel.h:27-33.
+ScannerF make_scanner(const strip_geometry& g) {
+  ScannerF s;
+  s.R = (float)g.radius;
+  s.L = (float)g.scintillator_length;
+  s.n_y = narrow16(g.n_y_pixels);
+  s.n_z = narrow16(g.n_z_pixels);
+  s.ph = (float)g.pixel_height;
+  s.pw = (float)g.pixel_width;
+  s.sz = (float)g.sigma_z;
+  s.sdl = (float)g.sigma_dl;
+  s.cy = (float)g.center_y;
+  s.cz = (float)g.center_z;
+  const float size_y = (float)s.n_y * s.ph;
+  const float size_z = (float)s.n_z * s.pw;
+  s.tl_y = s.cy + size_y / 2.0f;
+  s.tl_z = s.cz - size_z / 2.0f;
+  s.tl_y_half_h = s.tl_y - s.ph / 2.0f;
+  s.tl_z_half_w = s.tl_z + s.pw / 2.0f;
+  s.half_L = s.L / 2.0f;
+  s.ipsz = 1.0f / (s.sz * s.sz);
+  s.ipsdl = 1.0f / (s.sdl * s.sdl);
+  s.kc = (float)((1.0 / (2.0 * M_PI * M_PI)) *
+                 (double)sqrtf((s.ipsz * s.ipsz) * s.ipsdl));
+  return s;
+}
+
+KernelF make_kernel(double sigma_z, double sigma_dl) {
+  KernelF k;
+  const float sz = (float)sigma_z, sdl = (float)sigma_dl;
+  k.ipsz = 1.0f / (sz * sz);
+  k.ipsdl = 1.0f / (sdl * sdl);
+  k.kc = (float)((1.0 / (2.0 * M_PI * M_PI)) *
+                 (double)sqrtf((k.ipsz * k.ipsz) * k.ipsdl));
+  k.c1 = -kLog2e * k.ipsz;
+  return k;
+}
+
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+int set_device(strip_ctx* ctx) {
+  CK(cudaSetDevice(ctx->device));
+  return STRIP_OK;
+}
+
+// Chooses the tile size and halos for the largest event box, within the
+// shared memory available to 2 CTAs per SM.
+Tiling choose_tiling(const strip_ctx* ctx, int max_w, int max_h) {
+  const int n_z = ctx->s.n_z, n_y = ctx->s.n_y;
+  const int budget = std::min(ctx->smem_optin, 113 * 1024);
+  Tiling t{};
+  int TX = 32, TY = 32;
+  int HX = max_w / 2 + 2, HY = max_h / 2 + 2;
+  for (;;) {
+    const int WX = std::min(n_z, TX + 2 * HX), WY = std::min(n_y, TY + 2 * HY);
+    const int WS = WX | 1;
+    const int bytes = 2 * WY * WS * 4;
+    if (bytes <= budget || (HX <= 8 && HY <= 8)) {
+      t.TX = TX;
+      t.TY = TY;
+      t.HX = HX;
+      t.HY = HY;
+      t.WXmax = WX;
+      t.WYmax = WY;
+      t.WS = WS;
+      t.smem_bytes = bytes;
+      break;
+    }
+    if (TX > 16 || TY > 16) {
+      TX = TY = 16;
+      continue;
+    }
+    if (HX >= HY) HX = HX * 3 / 4; else HY = HY * 3 / 4;
+  }
+  t.ntx = (n_z + t.TX - 1) / t.TX;
+  t.nty = (n_y + t.TY - 1) / t.TY;
+  t.n_tiles = t.ntx * t.nty;
+  return t;
+}
+
+// Sorts events (device arrays; `orig` maps them to the caller's indices or is
+// null for identity) into (subset, tile) bins and builds the work items.
+// On success the context owns the new binned arrays.
+int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
+               const float* dl, const int64_t* orig, int64_t n,
+               int n_subsets) {
+  cudaStream_t st = ctx->stream;
+  cudaEventRecord(ctx->ev0, st);
+  int4* boxes = nullptr;
+  int* keys = nullptr;
+  int* d_wh = nullptr;
+  unsigned long long* d_empty = nullptr;
+  unsigned long long* d_hist = nullptr;
+  float *ozu = nullptr, *ozd = nullptr, *odl = nullptr;
+  int64_t* operm = nullptr;
+  auto cleanup = [&]() {
+    dfree(boxes);
+    dfree(keys);
+    dfree(d_wh);
+    dfree(d_empty);
+    dfree(d_hist);
+    dfree(ozu);
+    dfree(ozd);
+    dfree(odl);
+    dfree(operm);
+  };
+  int rc = STRIP_OK;
+#define CKB(call)                                                        \
+  do {                                                                   \
+    cudaError_t e_ = (call);                                             \
+    if (e_ != cudaSuccess) {                                             \
+      rc = fail(ctx, e_ == cudaErrorMemoryAllocation ? STRIP_E_NOMEM     \
+                                                     : STRIP_E_CUDA,     \
+                "%s: %s", #call, cudaGetErrorString(e_));                \
+      cleanup();                                                         \
+      return rc;                                                         \
+    }                                                                    \
+  } while (0)
+  const size_t nn = (size_t)std::max<int64_t>(n, 1);
+  CKB(cudaMalloc(&boxes, nn * sizeof(int4)));
+  CKB(cudaMalloc(&keys, nn * sizeof(int)));
+  CKB(cudaMalloc(&d_wh, 2 * sizeof(int)));
+  CKB(cudaMalloc(&d_empty, sizeof(unsigned long long)));
+  CKB(cudaMemsetAsync(d_wh, 0, 2 * sizeof(int), st));
+  CKB(cudaMemsetAsync(d_empty, 0, sizeof(unsigned long long), st));
+  CKB(launch_event_boxes(ctx->s, zu, zd, dl, n, boxes, d_wh, d_empty, st));
+  int wh[2] = {0, 0};
+  unsigned long long n_empty = 0;
+  CKB(cudaMemcpyAsync(wh, d_wh, sizeof wh, cudaMemcpyDeviceToHost, st));
+  CKB(cudaMemcpyAsync(&n_empty, d_empty, sizeof n_empty,
+                      cudaMemcpyDeviceToHost, st));
+  CKB(cudaStreamSynchronize(st));
+
+  const Tiling t = choose_tiling(ctx, wh[0], wh[1]);
+  const int n_keys = n_subsets * (t.n_tiles + 1);
+  CKB(cudaMalloc(&d_hist, (size_t)n_keys * sizeof(unsigned long long)));
+  CKB(cudaMemsetAsync(d_hist, 0, (size_t)n_keys * sizeof(unsigned long long),
+                      st));
+  CKB(launch_bin_keys(t, ctx->s.n_z, ctx->s.n_y, boxes, orig, n, n_subsets,
+                      keys, d_hist, st));
+  std::vector<unsigned long long> hist(n_keys), offs(n_keys);
+  CKB(cudaMemcpyAsync(hist.data(), d_hist, n_keys * sizeof(unsigned long long),
+                      cudaMemcpyDeviceToHost, st));
+  CKB(cudaStreamSynchronize(st));
+  unsigned long long total = 0;
+  for (int k = 0; k < n_keys; ++k) {
+    offs[k] = total;
+    total += hist[k];
+  }
+  const size_t nb = (size_t)std::max<unsigned long long>(total, 1);
+  CKB(cudaMalloc(&ozu, nb * sizeof(float)));
+  CKB(cudaMalloc(&ozd, nb * sizeof(float)));
+  CKB(cudaMalloc(&odl, nb * sizeof(float)));
+  CKB(cudaMalloc(&operm, nb * sizeof(int64_t)));
+  CKB(cudaMemcpyAsync(d_hist, offs.data(), n_keys * sizeof(unsigned long long),
+                      cudaMemcpyHostToDevice, st));
+  CKB(launch_bin_scatter(keys, n, zu, zd, dl, orig, d_hist, ozu, ozd, odl,
+                         operm, st));
+
+  // Work items: chunks of each (subset, tile) bin, sized for >= ~8 waves.
+  std::vector<WorkItem> items;
+  std::vector<int> ib(n_subsets), ic(n_subsets);
+  std::vector<int64_t> gb(n_subsets), gc(n_subsets);
+  const int64_t per_sub = (int64_t)(total / (unsigned long long)n_subsets) + 1;
+  const int64_t target = (int64_t)ctx->sm_count * 2 * 8;
+  const int64_t chunk =
+      std::min<int64_t>(1 << 15, std::max<int64_t>(64, per_sub / target + 1));
+  for (int sb = 0; sb < n_subsets; ++sb) {
+    ib[sb] = (int)items.size();
+    for (int tile = 0; tile < t.n_tiles; ++tile) {
+      const int key = sb * (t.n_tiles + 1) + tile;
+      int64_t b = (int64_t)offs[key], c = (int64_t)hist[key];
+      while (c > 0) {
+        const int64_t m = std::min(c, chunk);
+        items.push_back(WorkItem{tile, (int32_t)m, b});
+        b += m;
+        c -= m;
+      }
+    }
+    ic[sb] = (int)items.size() - ib[sb];
+    const int gkey = sb * (t.n_tiles + 1) + t.n_tiles;
+    gb[sb] = (int64_t)offs[gkey];
+    gc[sb] = (int64_t)hist[gkey];
+  }
+  WorkItem* d_items = nullptr;
+  CKB(cudaMalloc(&d_items, std::max<size_t>(items.size(), 1) * sizeof(WorkItem)));
+  if (!items.empty()) {
+    cudaError_t e = cudaMemcpyAsync(d_items, items.data(),
+                                    items.size() * sizeof(WorkItem),
+                                    cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) {
+      cudaFree(d_items);
+      CKB(e);
+    }
+  }
+  cudaEventRecord(ctx->ev1, st);
+  {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      cudaFree(d_items);
+      CKB(e);
+    }
+  }
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+
+  // commit
+  dfree(ctx->d_zu);
+  dfree(ctx->d_zd);
+  dfree(ctx->d_dl);
+  dfree(ctx->d_perm);
+  dfree(ctx->d_items);
+  ctx->d_zu = ozu;
+  ctx->d_zd = ozd;
+  ctx->d_dl = odl;
+  ctx->d_perm = operm;
+  ozu = ozd = odl = nullptr;
+  operm = nullptr;
+  ctx->d_items = d_items;
+  ctx->items.swap(items);
+  ctx->sub_item_begin.swap(ib);
+  ctx->sub_item_count.swap(ic);
+  ctx->sub_g_begin.swap(gb);
+  ctx->sub_g_count.swap(gc);
+  ctx->n_binned = (int64_t)total;
+  ctx->n_subsets = n_subsets;
+  ctx->t = t;
+  ctx->max_w = wh[0];
+  ctx->max_h = wh[1];
+  int64_t n_ovf = 0;
+  for (int sb = 0; sb < n_subsets; ++sb) n_ovf += ctx->sub_g_count[sb];
+  strip_stats& S = ctx->stats;
+  S.n_events = ctx->n_events;
+  S.n_empty = (int64_t)n_empty;
+  S.n_overflow = n_ovf;
+  S.n_tiles_z = t.ntx;
+  S.n_tiles_y = t.nty;
+  S.tile_z = t.TX;
+  S.tile_y = t.TY;
+  S.halo_z = t.HX;
+  S.halo_y = t.HY;
+  S.n_work_items = (int32_t)ctx->items.size();
+  S.n_subsets = n_subsets;
+  S.max_box_w = wh[0];
+  S.max_box_h = wh[1];
+  S.smem_bytes = t.smem_bytes;
+  S.last_setup_ms = ms;
+  cleanup();
+  return STRIP_OK;
+#undef CKB
+}
+
+int ensure_sens5(strip_ctx* ctx) {
+  if (ctx->d_sens5) return STRIP_OK;
+  CK(cudaMalloc(&ctx->d_sens5, ctx->n_pix * sizeof(float)));
+  CK(launch_sensitivity(ctx->s, 1, ctx->d_sens5, ctx->stream));
+  return STRIP_OK;
+}
+
+int check_ready(strip_ctx* ctx) {
+  if (!ctx) return STRIP_E_INVALID;
+  if (ctx->n_subsets <= 0)
+    return fail(ctx, STRIP_E_STATE, "no events: call strip_set_events first");
+  return STRIP_OK;
+}
+
+LaunchArgs base_args(strip_ctx* ctx) {
+  LaunchArgs a{};
+  a.s = ctx->s;
+  a.k = make_kernel(ctx->g.sigma_z, ctx->g.sigma_dl);
+  a.t = ctx->t;
+  a.zu = ctx->d_zu;
+  a.zd = ctx->d_zd;
+  a.dl = ctx->d_dl;
+  a.perm = ctx->d_perm;
+  a.rho = ctx->d_rho;
+  a.acc = ctx->d_acc;
+  a.status = ctx->d_status;
+  return a;
+}
+
+// Runs op over every subset's work items and global-path events.
+int run_all(strip_ctx* ctx, int op, int mode, LaunchArgs a) {
+  for (int sb = 0; sb < ctx->n_subsets; ++sb) {
+    a.items = ctx->d_items + ctx->sub_item_begin[sb];
+    a.n_items = ctx->sub_item_count[sb];
+    a.g_begin = ctx->sub_g_begin[sb];
+    a.g_count = ctx->sub_g_count[sb];
+    CK(launch_tile(op, mode, ctx->accum, a, ctx->stream));
+    CK(launch_global(op, mode, ctx->accum, a, ctx->stream));
+  }
+  return STRIP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int strip_ctx_create(const strip_geometry* g, int device, strip_ctx** out) {
+  if (!g || !out) return STRIP_E_INVALID;
+  *out = nullptr;
+  if (g->n_y_pixels <= 0 || g->n_z_pixels <= 0 || g->n_y_pixels > 32767 ||
+      g->n_z_pixels > 32767 || !(g->pixel_height > 0) ||
+      !(g->pixel_width > 0) || !(g->sigma_z > 0) || !(g->sigma_dl > 0) ||
+      !(g->radius > 0))
+    return STRIP_E_INVALID;
+  int n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev <= 0) {
+    cudaGetLastError();
+    return STRIP_E_NODEVICE;
+  }
+  if (device < 0 || device >= n_dev) return STRIP_E_INVALID;
+  strip_ctx* ctx = new (std::nothrow) strip_ctx();
+  if (!ctx) return STRIP_E_NOMEM;
+  ctx->device = device;
+  ctx->g = *g;
+  ctx->s = make_scanner(*g);
+  ctx->n_pix = (int64_t)ctx->s.n_y * ctx->s.n_z;
+  int rc = STRIP_OK;
+  do {
+    if (cudaSetDevice(device) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
+    snprintf(ctx->devname, sizeof ctx->devname, "%s", prop.name);
+    ctx->sm_count = prop.multiProcessorCount;
+    ctx->smem_optin = (int)prop.sharedMemPerBlockOptin;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
+    if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
+    if (cudaMalloc(&ctx->d_rho, ctx->n_pix * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_acc, ctx->n_pix * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_status, sizeof(int)) != cudaSuccess) { rc = STRIP_E_NOMEM; break; }
+    std::vector<float> ones((size_t)ctx->n_pix, 1.0f);  // reconstruction.h:59
+    if (cudaMemcpy(ctx->d_rho, ones.data(), ctx->n_pix * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(ctx->d_acc, 0, ctx->n_pix * sizeof(double)) != cudaSuccess ||
+        cudaMemset(ctx->d_status, 0, sizeof(int)) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
+  } while (0);
+  if (rc != STRIP_OK) {
+    cudaGetLastError();
+    strip_ctx_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return STRIP_OK;
+}
+
+int strip_ctx_destroy(strip_ctx* ctx) {
+  if (!ctx) return STRIP_E_INVALID;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  dfree(ctx->d_rho);
+  dfree(ctx->d_acc);
+  dfree(ctx->d_sens5);
+  dfree(ctx->d_zu);
+  dfree(ctx->d_zd);
+  dfree(ctx->d_dl);
+  dfree(ctx->d_perm);
+  dfree(ctx->d_items);
+  dfree(ctx->d_status);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  for (cudaEvent_t ev : ctx->tile_marks) cudaEventDestroy(ev);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return STRIP_OK;
+}
+
+int strip_last_error(const strip_ctx* ctx, char* buf, size_t size) {
+  if (!ctx || !buf || size == 0) return STRIP_E_INVALID;
+  snprintf(buf, size, "%s", ctx->err.c_str());
+  return STRIP_OK;
+}
+
+int strip_device_name(const strip_ctx* ctx, char* buf, size_t size) {
+  if (!ctx || !buf || size == 0) return STRIP_E_INVALID;
+  snprintf(buf, size, "%s", ctx->devname);
+  return STRIP_OK;
+}
+
+int strip_set_accumulation(strip_ctx* ctx, int accum) {
+  if (!ctx) return STRIP_E_INVALID;
+  if (accum < STRIP_ACCUM_FP32 || accum > STRIP_ACCUM_FP64)
+    return fail(ctx, STRIP_E_INVALID, "unknown accumulation %d", accum);
+  ctx->accum = accum;
+  return STRIP_OK;
+}
+
+int strip_get_stats(const strip_ctx* ctx, strip_stats* out) {
+  if (!ctx || !out) return STRIP_E_INVALID;
+  *out = ctx->stats;
+  return STRIP_OK;
+}
+
+int strip_set_events_device(strip_ctx* ctx, const float* zu, const float* zd,
+                            const float* dl, int64_t n, int n_subsets) {
+  if (!ctx) return STRIP_E_INVALID;
+  if (n < 0 || (n > 0 && (!zu || !zd || !dl)) || n_subsets < 1 ||
+      n_subsets > 4096)
+    return fail(ctx, STRIP_E_INVALID, "invalid events (n=%lld, subsets=%d)",
+                (long long)n, n_subsets);
+  if (int rc = set_device(ctx)) return rc;
+  ctx->n_events = n;
+  return bin_events(ctx, zu, zd, dl, nullptr, n, n_subsets);
+}
+
+int strip_set_events(strip_ctx* ctx, const float* zu, const float* zd,
+                     const float* dl, int64_t n, int n_subsets) {
+  if (!ctx) return STRIP_E_INVALID;
+  if (n < 0 || (n > 0 && (!zu || !zd || !dl)) || n_subsets < 1 ||
+      n_subsets > 4096)
+    return fail(ctx, STRIP_E_INVALID, "invalid events (n=%lld, subsets=%d)",
+                (long long)n, n_subsets);
+  if (int rc = set_device(ctx)) return rc;
+  float* d = nullptr;
+  const size_t bytes = (size_t)std::max<int64_t>(n, 1) * sizeof(float);
+  CK(cudaMalloc(&d, 3 * bytes));
+  float* dzu = d;
+  float* dzd = d + std::max<int64_t>(n, 1);
+  float* ddl = d + 2 * std::max<int64_t>(n, 1);
+  cudaError_t e = cudaSuccess;
+  if (n > 0) {
+    e = cudaMemcpyAsync(dzu, zu, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dzd, zd, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ddl, dl, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+  }
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    CK(e);
+  }
+  ctx->n_events = n;
+  int rc = bin_events(ctx, dzu, dzd, ddl, nullptr, n, n_subsets);
+  cudaFree(d);
+  return rc;
+}
+
+int strip_set_responses(strip_ctx* ctx, const float* t, int64_t n,
+                        int n_subsets) {
+  if (!ctx) return STRIP_E_INVALID;
+  if (n < 0 || (n > 0 && !t))
+    return fail(ctx, STRIP_E_INVALID, "invalid responses");
+  std::vector<float> zu((size_t)n), zd((size_t)n), dl((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {  // AoS -> SoA, gpu_events_soa.h:18-22
+    zu[i] = t[3 * i];
+    zd[i] = t[3 * i + 1];
+    dl[i] = t[3 * i + 2];
+  }
+  return strip_set_events(ctx, zu.data(), zd.data(), dl.data(), n, n_subsets);
+}
+
+int strip_set_image(strip_ctx* ctx, const float* rho) {
+  if (!ctx || !rho) return STRIP_E_INVALID;
+  if (int rc = set_device(ctx)) return rc;
+  CK(cudaMemcpyAsync(ctx->d_rho, rho, ctx->n_pix * sizeof(float),
+                     cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return STRIP_OK;
+}
+
+int strip_get_image(strip_ctx* ctx, float* rho) {
+  if (!ctx || !rho) return STRIP_E_INVALID;
+  if (int rc = set_device(ctx)) return rc;
+  CK(cudaMemcpyAsync(rho, ctx->d_rho, ctx->n_pix * sizeof(float),
+                     cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return STRIP_OK;
+}
+
+int strip_get_sensitivity(strip_ctx* ctx, int five_point, float* out) {
+  if (!ctx || !out) return STRIP_E_INVALID;
+  if (int rc = set_device(ctx)) return rc;
+  float* d = nullptr;
+  CK(cudaMalloc(&d, ctx->n_pix * sizeof(float)));
+  cudaError_t e = launch_sensitivity(ctx->s, five_point ? 1 : 0, d, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, d, ctx->n_pix * sizeof(float),
+                        cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d);
+  CK(e);
+  return STRIP_OK;
+}
+
+int strip_iterate(strip_ctx* ctx, int n_iter, int mode, int n_subsets,
+                  int first, strip_progress_cb progress, void* user) {
+  if (int rc = check_ready(ctx)) return rc;
+  if (n_iter < 0 || (mode != STRIP_MODE_CPU && mode != STRIP_MODE_GPU) ||
+      n_subsets < 1 || n_subsets > 4096)
+    return fail(ctx, STRIP_E_INVALID, "invalid iterate arguments");
+  if (int rc = set_device(ctx)) return rc;
+  if (n_subsets != ctx->n_subsets) {
+    // re-bin: the binned arrays become the input, perm keeps caller indices
+    float* zu = ctx->d_zu;
+    float* zd = ctx->d_zd;
+    float* dl = ctx->d_dl;
+    int64_t* pm = ctx->d_perm;
+    ctx->d_zu = ctx->d_zd = ctx->d_dl = nullptr;
+    ctx->d_perm = nullptr;
+    int rc = bin_events(ctx, zu, zd, dl, pm, ctx->n_binned, n_subsets);
+    if (rc != STRIP_OK) {
+      ctx->d_zu = zu;
+      ctx->d_zd = zd;
+      ctx->d_dl = dl;
+      ctx->d_perm = pm;
+      return rc;
+    }
+    cudaFree(zu);
+    cudaFree(zd);
+    cudaFree(dl);
+    cudaFree(pm);
+  }
+  if (mode == STRIP_MODE_GPU)
+    if (int rc = ensure_sens5(ctx)) return rc;
+  LaunchArgs a = base_args(ctx);
+  a.sens = (mode == STRIP_MODE_GPU) ? ctx->d_sens5 : nullptr;
+  int launches = 0;
+  // one event pair per tile launch, for the tile kernel's device time
+  const size_t n_marks = (size_t)n_iter * ctx->n_subsets;
+  while (ctx->tile_marks.size() < 2 * n_marks) {
+    cudaEvent_t ev;
+    CK(cudaEventCreate(&ev));
+    ctx->tile_marks.push_back(ev);
+  }
+  size_t mark = 0;
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  for (int it = 0; it < n_iter; ++it) {
+    if (progress) {
+      CK(cudaStreamSynchronize(ctx->stream));
+      progress(first + it, 0, user);
+    }
+    for (int sb = 0; sb < ctx->n_subsets; ++sb) {
+      a.items = ctx->d_items + ctx->sub_item_begin[sb];
+      a.n_items = ctx->sub_item_count[sb];
+      a.g_begin = ctx->sub_g_begin[sb];
+      a.g_count = ctx->sub_g_count[sb];
+      CK(cudaEventRecord(ctx->tile_marks[2 * mark], ctx->stream));
+      CK(launch_tile(OP_MLEM, mode, ctx->accum, a, ctx->stream));
+      CK(cudaEventRecord(ctx->tile_marks[2 * mark + 1], ctx->stream));
+      ++mark;
+      CK(launch_global(OP_MLEM, mode, ctx->accum, a, ctx->stream));
+      CK(launch_update(ctx->d_rho, ctx->d_acc, ctx->n_pix,
+                       (double)ctx->n_subsets, ctx->stream));
+      launches += (a.n_items > 0) + (a.g_count > 0) + 1;
+    }
+    if (progress) {
+      CK(cudaStreamSynchronize(ctx->stream));
+      if (progress(first + it, 1, user)) {
+        ++it;
+        break;
+      }
+    }
+  }
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  double tile_ms = 0;
+  for (size_t m = 0; m < mark; ++m) {
+    float t = 0;
+    if (cudaEventElapsedTime(&t, ctx->tile_marks[2 * m],
+                             ctx->tile_marks[2 * m + 1]) == cudaSuccess)
+      tile_ms += t;
+  }
+  ctx->stats.last_iterate_ms = ms;
+  ctx->stats.last_tile_ms = tile_ms;
+  ctx->stats.kernel_launches = launches;
+  return STRIP_OK;
+}
+
+int strip_forward(strip_ctx* ctx, const float* rho, double sigma_z,
+                  double sigma_dl, int mode, double* y) {
+  if (int rc = check_ready(ctx)) return rc;
+  if (!rho || !y || !(sigma_z > 0) || !(sigma_dl > 0) ||
+      (mode != STRIP_MODE_CPU && mode != STRIP_MODE_GPU))
+    return fail(ctx, STRIP_E_INVALID, "invalid forward arguments");
+  if (int rc = set_device(ctx)) return rc;
+  if (mode == STRIP_MODE_GPU)
+    if (int rc = ensure_sens5(ctx)) return rc;
+  float* d_img = nullptr;
+  double* d_y = nullptr;
+  CK(cudaMalloc(&d_img, ctx->n_pix * sizeof(float)));
+  cudaError_t e = cudaMalloc(&d_y, std::max<int64_t>(ctx->n_events, 1) * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_img, rho, ctx->n_pix * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_y, 0, std::max<int64_t>(ctx->n_events, 1) * sizeof(double), ctx->stream);
+  int rc = STRIP_OK;
+  if (e == cudaSuccess) {
+    LaunchArgs a = base_args(ctx);
+    a.k = make_kernel(sigma_z, sigma_dl);
+    a.rho = d_img;
+    a.sens = (mode == STRIP_MODE_GPU) ? ctx->d_sens5 : nullptr;
+    a.y_out = d_y;
+    rc = run_all(ctx, OP_FORWARD, mode, a);
+    if (rc == STRIP_OK && ctx->n_events > 0)
+      e = cudaMemcpyAsync(y, d_y, ctx->n_events * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  }
+  cudaFree(d_img);
+  cudaFree(d_y);
+  if (rc != STRIP_OK) return rc;
+  CK(e);
+  return STRIP_OK;
+}
+
+int strip_adjoint(strip_ctx* ctx, const double* w, double sigma_z,
+                  double sigma_dl, int mode, double* g) {
+  if (int rc = check_ready(ctx)) return rc;
+  if (!w || !g || !(sigma_z > 0) || !(sigma_dl > 0) ||
+      (mode != STRIP_MODE_CPU && mode != STRIP_MODE_GPU))
+    return fail(ctx, STRIP_E_INVALID, "invalid adjoint arguments");
+  if (int rc = set_device(ctx)) return rc;
+  if (mode == STRIP_MODE_GPU)
+    if (int rc = ensure_sens5(ctx)) return rc;
+  double* d_w = nullptr;
+  double* d_acc = nullptr;
+  double* d_out = nullptr;
+  const int64_t ne = std::max<int64_t>(ctx->n_events, 1);
+  cudaError_t e = cudaMalloc(&d_w, ne * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&d_acc, ctx->n_pix * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&d_out, ctx->n_pix * sizeof(double));
+  if (e == cudaSuccess && ctx->n_events > 0)
+    e = cudaMemcpyAsync(d_w, w, ctx->n_events * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_acc, 0, ctx->n_pix * sizeof(double), ctx->stream);
+  int rc = STRIP_OK;
+  if (e == cudaSuccess) {
+    LaunchArgs a = base_args(ctx);
+    a.k = make_kernel(sigma_z, sigma_dl);
+    a.acc = d_acc;
+    a.w_in = d_w;
+    rc = run_all(ctx, OP_ADJOINT, mode, a);
+    if (rc == STRIP_OK)
+      e = launch_scale_copy(d_acc, mode == STRIP_MODE_GPU ? ctx->d_sens5 : nullptr, d_out, ctx->n_pix, ctx->stream);
+    if (rc == STRIP_OK && e == cudaSuccess)
+      e = cudaMemcpyAsync(g, d_out, ctx->n_pix * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  }
+  cudaFree(d_w);
+  cudaFree(d_acc);
+  cudaFree(d_out);
+  if (rc != STRIP_OK) return rc;
+  CK(e);
+  return STRIP_OK;
+}
+
+int strip_grad_sigma(strip_ctx* ctx, const float* rho, const double* w,
+                     double sigma_z, double sigma_dl, double* d_sigma_z,
+                     double* d_sigma_dl) {
+  (void)rho;
+  (void)w;
+  (void)sigma_z;
+  (void)sigma_dl;
+  (void)d_sigma_z;
+  (void)d_sigma_dl;
+  return fail(ctx, STRIP_E_STATE, "strip_grad_sigma: not available yet");
+}
+
+int strip_count_work(strip_ctx* ctx, int64_t* n_bb, int64_t* n_in,
+                     int64_t* n_nonempty) {
+  if (int rc = check_ready(ctx)) return rc;
+  if (int rc = set_device(ctx)) return rc;
+  unsigned long long* d = nullptr;
+  CK(cudaMalloc(&d, 3 * sizeof(unsigned long long)));
+  unsigned long long h[3] = {0, 0, 0};
+  cudaError_t e = cudaMemsetAsync(d, 0, sizeof h, ctx->stream);
+  if (e == cudaSuccess)
+    e = launch_count_work(ctx->s, ctx->d_zu, ctx->d_zd, ctx->d_dl,
+                          ctx->n_binned, d, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d);
+  CK(e);
+  if (n_bb) *n_bb = (int64_t)h[0];
+  if (n_in) *n_in = (int64_t)h[1];
+  if (n_nonempty) *n_nonempty = (int64_t)h[2];
+  return STRIP_OK;
+}
+
+int strip_probe_fp32_peak(int device, double* tflops) {
+  if (!tflops) return STRIP_E_INVALID;
+  strip_ctx* ctx = nullptr;  // for CK (no message storage)
+  int n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev <= 0) {
+    cudaGetLastError();
+    return STRIP_E_NODEVICE;
+  }
+  CK(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, device));
+  float* out = nullptr;
+  CK(cudaMalloc(&out, prop.multiProcessorCount * 4 * sizeof(float)));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  double best = 0, flops = 0;
+  cudaError_t err = cudaSuccess;
+  for (int rep = 0; rep < 4 && err == cudaSuccess; ++rep) {
+    cudaEventRecord(e0, 0);
+    err = launch_fma_peak(prop.multiProcessorCount, 4096, out, &flops, 0);
+    cudaEventRecord(e1, 0);
+    if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0 && ms > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  CK(err);
+  *tflops = best;
+  return STRIP_OK;
+}
+
+int strip_debug_pixel_sets(strip_ctx* ctx, const float* zu, const float* zd,
+                           const float* dl, int64_t n, int32_t* n_bb,
+                           int32_t* n_in, uint64_t* digest) {
+  if (!ctx) return STRIP_E_INVALID;
+  if (n < 0 || (n > 0 && (!zu || !zd || !dl)))
+    return fail(ctx, STRIP_E_INVALID, "invalid events");
+  if (n == 0) return STRIP_OK;
+  if (int rc = set_device(ctx)) return rc;
+  char* d = nullptr;
+  const size_t fb = n * sizeof(float);
+  const size_t need = 3 * fb + 2 * n * sizeof(int32_t) + n * sizeof(uint64_t) + 64;
+  CK(cudaMalloc(&d, need));
+  float* dzu = (float*)d;
+  float* dzd = dzu + n;
+  float* ddl = dzd + n;
+  uint64_t* ddg = (uint64_t*)(((uintptr_t)(ddl + n) + 15) & ~(uintptr_t)15);
+  int32_t* dbb = (int32_t*)(ddg + n);
+  int32_t* din = dbb + n;
+  cudaError_t e = cudaMemcpyAsync(dzu, zu, fb, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dzd, zd, fb, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ddl, dl, fb, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = launch_debug_sets(ctx->s, dzu, dzd, ddl, n, dbb, din, ddg, ctx->stream);
+  if (e == cudaSuccess && n_bb) e = cudaMemcpyAsync(n_bb, dbb, n * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess && n_in) e = cudaMemcpyAsync(n_in, din, n * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess && digest) e = cudaMemcpyAsync(digest, ddg, n * sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d);
+  CK(e);
+  return STRIP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,112 @@
+// Internal interfaces between the C-ABI layer (strip_capi.cu) and the
+// kernels (strip_kernels.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "stripmlem.h"
+#include "strip_device.cuh"
+#include "strip_kernel_eval.cuh"
+
+namespace stripmlem {
+
+// A unit of work of the tile kernel: `count` events starting at sorted
+// position `begin`, all of whose boxes lie inside the window of `tile`.
+struct WorkItem {
+  int32_t tile;
+  int32_t count;
+  int64_t begin;
+};
+
+// Image tiling.  Tile (bx, by) owns pixels [bx*TX, (bx+1)*TX) x [by*TY, ...);
+// its shared-memory window adds a halo of (HX, HY) pixels on each side,
+// clamped to the image.  WXmax/WYmax bound every window, WS is the padded
+// shared-memory row stride.
+struct Tiling {
+  int TX, TY, HX, HY, ntx, nty, n_tiles;
+  int WXmax, WYmax, WS;
+  int smem_bytes;
+};
+
+__host__ __device__ inline void tile_window(const Tiling& t, int n_z, int n_y,
+                                            int tile, int& wx0, int& wy0,
+                                            int& wx1, int& wy1) {
+  const int bx = tile % t.ntx, by = tile / t.ntx;
+  wx0 = bx * t.TX - t.HX;
+  wx0 = wx0 < 0 ? 0 : wx0;
+  wy0 = by * t.TY - t.HY;
+  wy0 = wy0 < 0 ? 0 : wy0;
+  wx1 = (bx + 1) * t.TX + t.HX;
+  wx1 = wx1 > n_z ? n_z : wx1;
+  wy1 = (by + 1) * t.TY + t.HY;
+  wy1 = wy1 > n_y ? n_y : wy1;
+}
+
+// What a tile / global-path launch computes.
+enum Op {
+  OP_MLEM = 0,     // D_e, then acc_j += K_ej / D_e
+  OP_FORWARD = 1,  // y_e = D_e
+  OP_ADJOINT = 2,  // acc_j += K_ej * w_e
+  OP_GRAD = 3      // d/dsigma of sum_e w_e D_e
+};
+
+struct LaunchArgs {
+  ScannerF s;
+  KernelF k;          // kernel constants (model sigmas)
+  Tiling t;
+  const float* zu;    // events, binned order
+  const float* zd;
+  const float* dl;
+  const int64_t* perm;   // binned position -> caller's event index
+  const float* rho;      // image
+  const float* sens;     // pixel sensitivity (gpu mode) or null
+  double* acc;           // backprojection accumulator (binary64)
+  const WorkItem* items;
+  int n_items;
+  int64_t g_begin;       // global-path event range [g_begin, g_begin+g_count)
+  int64_t g_count;
+  double* y_out;         // OP_FORWARD: per event (caller order)
+  const double* w_in;    // OP_ADJOINT / OP_GRAD: per event weights (caller order)
+  double* grad_out;      // OP_GRAD: 2 doubles (atomic)
+  float sz, sdl;         // OP_GRAD: model sigmas
+  int* status;           // device status word (0 = ok)
+};
+
+// ---- launchers (strip_kernels.cu) ----------------------------------------
+cudaError_t launch_event_boxes(const ScannerF& s, const float* zu,
+                               const float* zd, const float* dl, int64_t n,
+                               int4* boxes, int* max_wh, unsigned long long* n_empty,
+                               cudaStream_t st);
+cudaError_t launch_bin_keys(const Tiling& t, int n_z, int n_y, const int4* boxes,
+                            const int64_t* orig, int64_t n, int n_subsets,
+                            int* keys, unsigned long long* hist,
+                            cudaStream_t st);
+cudaError_t launch_bin_scatter(const int* keys, int64_t n, const float* zu,
+                               const float* zd, const float* dl,
+                               const int64_t* orig,
+                               unsigned long long* cursor, float* ozu,
+                               float* ozd, float* odl, int64_t* operm,
+                               cudaStream_t st);
+cudaError_t launch_tile(int op, int mode, int accum, const LaunchArgs& a,
+                        cudaStream_t st);
+cudaError_t launch_global(int op, int mode, int accum, const LaunchArgs& a,
+                          cudaStream_t st);
+cudaError_t launch_update(float* rho, double* acc, int64_t n_pix, double scale,
+                          cudaStream_t st);
+cudaError_t launch_sensitivity(const ScannerF& s, int five_point, float* out,
+                               cudaStream_t st);
+cudaError_t launch_debug_sets(const ScannerF& s, const float* zu,
+                              const float* zd, const float* dl, int64_t n,
+                              int32_t* n_bb, int32_t* n_in, uint64_t* digest,
+                              cudaStream_t st);
+cudaError_t launch_scale_copy(const double* acc, const float* sens,
+                              double* out, int64_t n_pix, cudaStream_t st);
+cudaError_t launch_count_work(const ScannerF& s, const float* zu,
+                              const float* zd, const float* dl, int64_t n,
+                              unsigned long long* out, cudaStream_t st);
+cudaError_t launch_fma_peak(int n_sm, int iters, float* out, double* flops,
+                            cudaStream_t st);
+
+}  // namespace stripmlem

@@ -1,0 +1,101 @@
+// Kernel values of the strip TOF model, factored by pixel row.
+//
+// For an event (y, tan, sec) and a pixel at distance (dz, dy) the reference
+// evaluates (gaussian_kernel.h:51-79)
+//     K = kc / sqrt(a'S a) * exp(-b'S b / 2),    S = diag(ipsz, ipsz, ipsdl)
+//     a = (-(yp-R) sec^2, -(yp+R) sec^2, -2 yp sec tan),  yp = dy + y
+//     b = (dz - dy tan, dz - dy tan, -2 dy sec)
+// a depends on the row only, and b'S b = 2 ipsz (dz - dy tan)^2 + ipsdl b_r^2,
+// so per row we keep pref = kc / sqrt(a'S a) and the constant part of the
+// exponent, and per pixel K = pref * 2^(c1 * t^2 + c0) with t = dz - dy tan.
+// AnalyticKernel (analytic_kernel.h:28-62) adds the o-vector: norm and b'S a
+// become linear in t, so it keeps three row constants more and needs a
+// reciprocal and a reciprocal square root per pixel.
+#pragma once
+
+namespace stripmlem {
+
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+constexpr float kLog2e = 1.4426950408889634f;
+
+// Kernel constants for given sigmas (the sigmas of the model, which may differ
+// from the geometry's sigmas that fix the pixel sets).
+struct KernelF {
+  float ipsz, ipsdl, kc;
+  float c1;  // -log2(e) * ipsz
+};
+
+// GaussianKernel, one row.
+struct GaussRow {
+  float pref, c0, dytan;
+  __device__ __forceinline__ void init(const KernelF& k, float R, float y,
+                                       float tan, float sec, float dy) {
+    const float sec_sq = sec * sec;
+    const float yp = dy + y;
+    const float ap = -(yp - R) * sec_sq;
+    const float aq = -(yp + R) * sec_sq;
+    const float ar = -2.0f * yp * sec * tan;
+    const float norm = k.ipsz * (ap * ap + aq * aq) + k.ipsdl * (ar * ar);
+    const float br = -2.0f * dy * sec;
+    pref = k.kc * rsqrt_approx(norm);
+    c0 = -0.5f * kLog2e * k.ipsdl * (br * br);
+    dytan = dy * tan;
+  }
+  __device__ __forceinline__ float eval(const KernelF& k, float dz) const {
+    const float t = dz - dytan;
+    return pref * ex2_approx(fmaf(k.c1, t * t, c0));
+  }
+};
+
+// AnalyticKernel, one row:  with t = dz - dy tan
+//   norm  = a'Sa + 2 o'Sb = n0 + n1 t
+//   b'Sa  = u1 t + u0
+//   b'Sb  = 2 ipsz t^2 + cr
+//   K     = kc / sqrt(norm) * exp(-(b'Sb - (b'Sa)^2 / norm) / 2)
+struct AnalyticRow {
+  float n0, n1, u0, u1, cr, dytan;
+  __device__ __forceinline__ void init(const KernelF& k, float R, float y,
+                                       float tan, float sec, float dy) {
+    const float sec_sq = sec * sec;
+    const float yp = dy + y;
+    const float ap = -(yp - R) * sec_sq;
+    const float aq = -(yp + R) * sec_sq;
+    const float ar = -2.0f * yp * sec * tan;
+    const float orr = -yp * sec * (1.0f + 2.0f * tan * tan);
+    const float br = -2.0f * dy * sec;
+    const float naa = k.ipsz * (ap * ap + aq * aq) + k.ipsdl * (ar * ar);
+    const float v1 = k.ipsz * tan * (ap + aq);
+    const float v0 = k.ipsdl * orr * br;
+    n0 = naa + 2.0f * v0;
+    n1 = 2.0f * v1;
+    u1 = k.ipsz * (ap + aq);
+    u0 = k.ipsdl * br * ar;
+    cr = k.ipsdl * (br * br);
+    dytan = dy * tan;
+  }
+  __device__ __forceinline__ float eval(const KernelF& k, float dz) const {
+    const float t = dz - dytan;
+    const float norm = fmaf(n1, t, n0);
+    const float bia = fmaf(u1, t, u0);
+    const float bib = fmaf(2.0f * k.ipsz, t * t, cr);
+    const float arg = -0.5f * kLog2e * (bib - bia * bia * rcp_approx(norm));
+    return k.kc * rsqrt_approx(norm) * ex2_approx(arg);
+  }
+};
+
+}  // namespace stripmlem

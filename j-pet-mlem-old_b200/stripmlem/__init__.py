@@ -1,0 +1,326 @@
+"""Python host side of the B200 strip list-mode TOF MLEM library.
+
+Mirrors the reference's operator interface for the 2D strip path
+(JPETTomography/j-pet-mlem-old):
+
+* ``Scanner``        -- Scanner<F, S> constructor arguments (src/2d/strip/scanner.h:39-67)
+* ``Reconstruction`` -- Reconstruction<F, Kernel>: ``rho``, ``sensitivity``,
+  ``responses`` and ``__call__(progress, n_iterations, n_iterations_so_far)``
+  (src/2d/strip/reconstruction.h:42-154)
+* ``run``            -- PET2D::Strip::GPU::Reconstruction::run with its output /
+  progress / device-name callbacks (src/2d/strip/cuda/reconstruction.cu:32-113)
+
+Everything calls the C ABI of lib/libstripmlem.so (include/stripmlem.h); the
+arithmetic runs in the library's sm_100a kernels.  Errors raise StripError.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import (ACCUM_FP32, ACCUM_FP64, ACCUM_KAHAN, MODE_CPU, MODE_GPU,
+                   STRIP_OK)
+
+__all__ = [
+    "Scanner", "Reconstruction", "StripError", "run", "generate_events",
+    "MODE_CPU", "MODE_GPU", "ACCUM_FP32", "ACCUM_KAHAN", "ACCUM_FP64",
+]
+
+
+class StripError(RuntimeError):
+    def __init__(self, code, message=""):
+        self.code = code
+        name = _lib.ERROR_NAMES.get(code, f"error {code}")
+        super().__init__(f"{name}: {message}" if message else name)
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Scanner:
+    """Scanner parameters (scanner.h:39-67 argument order).
+
+    ``Scanner(radius, scintillator_length, n_y_pixels, n_z_pixels,
+    pixel_height, pixel_width, sigma_z, sigma_dl, center_y=0, center_z=0)``
+    """
+
+    def __init__(self, radius, scintillator_length, n_y_pixels, n_z_pixels,
+                 pixel_height, pixel_width, sigma_z, sigma_dl, center_y=0.0,
+                 center_z=0.0):
+        self.radius = float(radius)
+        self.scintillator_length = float(scintillator_length)
+        self.n_y_pixels = int(n_y_pixels)
+        self.n_z_pixels = int(n_z_pixels)
+        self.pixel_height = float(pixel_height)
+        self.pixel_width = float(pixel_width)
+        self.sigma_z = float(sigma_z)
+        self.sigma_dl = float(sigma_dl)
+        self.center_y = float(center_y)
+        self.center_z = float(center_z)
+
+    @classmethod
+    def from_cli(cls, radius, length, s_pixel, s_z, s_dl, n_z_pixels=None,
+                 n_y_pixels=None, n_pixels=None):
+        """calculate_scanner_options + PET2D_STRIP_SCANNER_CL
+        (options.cpp:106-124, options.h:42-50)."""
+        import math
+        if n_pixels:
+            n_z_pixels = n_y_pixels = n_pixels
+        if not n_z_pixels:
+            n_z_pixels = int(math.ceil(length / s_pixel))
+        if not n_y_pixels:
+            n_y_pixels = int(math.ceil(2 * radius / s_pixel))
+        return cls(radius, length, n_y_pixels, n_z_pixels, s_pixel, s_pixel,
+                   s_z, s_dl)
+
+    @property
+    def total_n_pixels(self):
+        return self.n_y_pixels * self.n_z_pixels
+
+    def geometry(self):
+        return _lib.Geometry(self.radius, self.scintillator_length,
+                             self.n_y_pixels, self.n_z_pixels,
+                             self.pixel_height, self.pixel_width,
+                             self.sigma_z, self.sigma_dl, self.center_y,
+                             self.center_z)
+
+    def as_dict(self):
+        return dict(vars(self))
+
+
+class Reconstruction:
+    """List-mode MLEM on the strip scanner, run by the library's kernels.
+
+    ``mode`` selects the reference's CPU semantics (MODE_CPU: GaussianKernel,
+    no sensitivity) or its ``--gpu`` semantics (MODE_GPU: AnalyticKernel with
+    the 5-point pixel sensitivity in the denominator).
+    """
+
+    def __init__(self, scanner, device=0, mode=MODE_CPU, accumulation=ACCUM_KAHAN):
+        self.lib = _lib.load()
+        self.scanner = scanner
+        self.mode = mode
+        self._geom = scanner.geometry()
+        ctx = ctypes.c_void_p()
+        rc = self.lib.strip_ctx_create(ctypes.byref(self._geom), int(device),
+                                       ctypes.byref(ctx))
+        if rc != STRIP_OK:
+            raise StripError(rc, "strip_ctx_create")
+        self._ctx = ctx
+        self.n_events = 0
+        self.n_subsets = 1
+        self._check(self.lib.strip_set_accumulation(self._ctx, accumulation))
+
+    # -- plumbing ---------------------------------------------------------
+    def _check(self, rc):
+        if rc != STRIP_OK:
+            buf = ctypes.create_string_buffer(512)
+            if self._ctx:
+                self.lib.strip_last_error(self._ctx, buf, 512)
+            raise StripError(rc, buf.value.decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self.lib.strip_ctx_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def device_name(self):
+        buf = ctypes.create_string_buffer(256)
+        self._check(self.lib.strip_device_name(self._ctx, buf, 256))
+        return buf.value.decode()
+
+    def stats(self):
+        s = _lib.Stats()
+        self._check(self.lib.strip_get_stats(self._ctx, ctypes.byref(s)))
+        return {name: getattr(s, name) for name, _ in s._fields_}
+
+    def set_accumulation(self, accum):
+        self._check(self.lib.strip_set_accumulation(self._ctx, int(accum)))
+
+    # -- events -----------------------------------------------------------
+    def set_events(self, z_u, z_d, dl, n_subsets=1):
+        z_u = np.ascontiguousarray(z_u, dtype=np.float32)
+        z_d = np.ascontiguousarray(z_d, dtype=np.float32)
+        dl = np.ascontiguousarray(dl, dtype=np.float32)
+        n = z_u.shape[0]
+        if z_d.shape[0] != n or dl.shape[0] != n:
+            raise StripError(_lib.STRIP_E_INVALID, "z_u, z_d, dl sizes differ")
+        self._check(self.lib.strip_set_events(self._ctx, _fp(z_u), _fp(z_d),
+                                              _fp(dl), n, int(n_subsets)))
+        self.n_events = n
+        self.n_subsets = int(n_subsets)
+
+    def set_events_device(self, z_u, z_d, dl, n_subsets=1):
+        """Device tensors (torch, float32, contiguous, same device)."""
+        n = int(z_u.numel())
+        self._check(self.lib.strip_set_events_device(
+            self._ctx, z_u.data_ptr(), z_d.data_ptr(), dl.data_ptr(), n,
+            int(n_subsets)))
+        self.n_events = n
+        self.n_subsets = int(n_subsets)
+
+    @property
+    def responses(self):
+        raise AttributeError("responses live on the device; keep the host copy")
+
+    @responses.setter
+    def responses(self, triples):
+        t = np.ascontiguousarray(triples, dtype=np.float32).reshape(-1, 3)
+        self._check(self.lib.strip_set_responses(self._ctx, _fp(t), t.shape[0],
+                                                 self.n_subsets))
+        self.n_events = t.shape[0]
+
+    # -- image ------------------------------------------------------------
+    @property
+    def rho(self):
+        out = np.empty((self.scanner.n_y_pixels, self.scanner.n_z_pixels), np.float32)
+        self._check(self.lib.strip_get_image(self._ctx, _fp(out)))
+        return out
+
+    @rho.setter
+    def rho(self, image):
+        img = np.ascontiguousarray(image, dtype=np.float32).reshape(
+            self.scanner.n_y_pixels, self.scanner.n_z_pixels)
+        self._check(self.lib.strip_set_image(self._ctx, _fp(img)))
+
+    def sensitivity(self, five_point=False):
+        out = np.empty((self.scanner.n_y_pixels, self.scanner.n_z_pixels), np.float32)
+        self._check(self.lib.strip_get_sensitivity(self._ctx, int(bool(five_point)), _fp(out)))
+        return out
+
+    # -- reconstruction ---------------------------------------------------
+    def __call__(self, progress=None, n_iterations=1, n_iterations_so_far=0,
+                 n_subsets=None, mode=None):
+        """Reconstruction::operator() (reconstruction.h:109-154)."""
+        if n_subsets is None:
+            n_subsets = self.n_subsets
+        if mode is None:
+            mode = self.mode
+        if progress is None:
+            cb = _lib.PROGRESS_CB()
+        else:
+            def _cb(completed, finished, _user):
+                r = progress(completed, bool(finished))
+                return 1 if r is True else 0
+            cb = _lib.PROGRESS_CB(_cb)
+        self._check(self.lib.strip_iterate(self._ctx, int(n_iterations), int(mode),
+                                           int(n_subsets), int(n_iterations_so_far),
+                                           cb, None))
+        self.n_subsets = int(n_subsets)
+
+    iterate = __call__
+
+    # -- projections ------------------------------------------------------
+    def forward(self, rho, sigma_z=None, sigma_dl=None, mode=None):
+        sz = self.scanner.sigma_z if sigma_z is None else float(sigma_z)
+        sdl = self.scanner.sigma_dl if sigma_dl is None else float(sigma_dl)
+        img = np.ascontiguousarray(rho, dtype=np.float32)
+        y = np.empty(self.n_events, np.float64)
+        self._check(self.lib.strip_forward(self._ctx, _fp(img), sz, sdl,
+                                           self.mode if mode is None else mode, _dp(y)))
+        return y
+
+    def adjoint(self, w, sigma_z=None, sigma_dl=None, mode=None):
+        sz = self.scanner.sigma_z if sigma_z is None else float(sigma_z)
+        sdl = self.scanner.sigma_dl if sigma_dl is None else float(sigma_dl)
+        wv = np.ascontiguousarray(w, dtype=np.float64)
+        g = np.empty((self.scanner.n_y_pixels, self.scanner.n_z_pixels), np.float64)
+        self._check(self.lib.strip_adjoint(self._ctx, _dp(wv), sz, sdl,
+                                           self.mode if mode is None else mode, _dp(g)))
+        return g
+
+    def grad_sigma(self, rho, w, sigma_z=None, sigma_dl=None):
+        sz = self.scanner.sigma_z if sigma_z is None else float(sigma_z)
+        sdl = self.scanner.sigma_dl if sigma_dl is None else float(sigma_dl)
+        img = np.ascontiguousarray(rho, dtype=np.float32)
+        wv = np.ascontiguousarray(w, dtype=np.float64)
+        gz = ctypes.c_double()
+        gd = ctypes.c_double()
+        self._check(self.lib.strip_grad_sigma(self._ctx, _fp(img), _dp(wv), sz, sdl,
+                                              ctypes.byref(gz), ctypes.byref(gd)))
+        return gz.value, gd.value
+
+    # -- parity -----------------------------------------------------------
+    def pixel_sets(self, z_u, z_d, dl):
+        z_u = np.ascontiguousarray(z_u, dtype=np.float32)
+        z_d = np.ascontiguousarray(z_d, dtype=np.float32)
+        dl = np.ascontiguousarray(dl, dtype=np.float32)
+        n = z_u.shape[0]
+        nbb = np.empty(n, np.int32)
+        nin = np.empty(n, np.int32)
+        dig = np.empty(n, np.uint64)
+        P = ctypes.POINTER
+        self._check(self.lib.strip_debug_pixel_sets(
+            self._ctx, _fp(z_u), _fp(z_d), _fp(dl), n,
+            nbb.ctypes.data_as(P(ctypes.c_int32)),
+            nin.ctypes.data_as(P(ctypes.c_int32)),
+            dig.ctypes.data_as(P(ctypes.c_uint64))))
+        return nbb, nin, dig
+
+
+def generate_events(scanner, ellipses, n, seed=1):
+    """Seeded synthetic events (strip_generate_events); returns z_u, z_d, dl.
+
+    ``ellipses``: iterable of (z, y, a, b, angle_deg, activity), the
+    reference's phantom-file ellipse fields, first on top.
+    """
+    lib = _lib.load()
+    el = list(ellipses)
+    arr = (_lib.Ellipse * len(el))(*[_lib.Ellipse(*map(float, e)) for e in el])
+    zu = np.empty(n, np.float32)
+    zd = np.empty(n, np.float32)
+    dl = np.empty(n, np.float32)
+    g = scanner.geometry()
+    rc = lib.strip_generate_events(ctypes.byref(g), arr, len(el), int(seed), int(n),
+                                   _fp(zu), _fp(zd), _fp(dl))
+    if rc != STRIP_OK:
+        raise StripError(rc, "strip_generate_events")
+    return zu, zd, dl
+
+
+def run(scanner, responses, rho, n_blocks, n_iterations_in_block, output=None,
+        progress=None, device=0, device_name=None, mode=MODE_GPU):
+    """GPU::Reconstruction::run (cuda/reconstruction.cu:32-113): runs
+    n_blocks x n_iterations_in_block iterations, calls output(-1, sensitivity)
+    first, output(i + 1, rho) after iterations 1-5, 10, 15, 20, 30, 50, 100 of
+    the first block and output((block + 1) * n, rho) after each block; rho is
+    updated in place."""
+    with Reconstruction(scanner, device=device, mode=mode) as rec:
+        if device_name is not None:
+            device_name(rec.device_name)
+        if output is not None:
+            output(-1, rec.sensitivity(five_point=True))
+        t = np.ascontiguousarray(responses, dtype=np.float32).reshape(-1, 3)
+        rec.set_events(t[:, 0], t[:, 1], t[:, 2])
+        rec.rho = rho
+        for block in range(n_blocks):
+            for i in range(n_iterations_in_block):
+                it = block * n_iterations_in_block + i
+                rec(progress, 1, it)
+                if (output is not None and block == 0 and i < n_iterations_in_block - 1
+                        and (i < 5 or i in (9, 14, 19, 29, 49, 99))):
+                    output(i + 1, rec.rho)
+            if output is not None:
+                output((block + 1) * n_iterations_in_block, rec.rho)
+        rho[...] = rec.rho.reshape(rho.shape)
+        if progress is not None:
+            progress(n_blocks * n_iterations_in_block, False)
+    return rho

@@ -1,0 +1,152 @@
+"""ctypes binding of the C ABI in include/stripmlem.h (lib/libstripmlem.so).
+
+The library is the product: if it is missing the import fails loudly; there
+is no CPU fallback.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libstripmlem.so")
+
+STRIP_OK = 0
+STRIP_E_INVALID = -1
+STRIP_E_CUDA = -2
+STRIP_E_NOMEM = -3
+STRIP_E_STATE = -4
+STRIP_E_KERNEL = -5
+STRIP_E_NODEVICE = -6
+
+MODE_CPU = 0
+MODE_GPU = 1
+ACCUM_FP32 = 0
+ACCUM_KAHAN = 1
+ACCUM_FP64 = 2
+
+ERROR_NAMES = {
+    STRIP_E_INVALID: "invalid argument",
+    STRIP_E_CUDA: "CUDA error",
+    STRIP_E_NOMEM: "out of memory",
+    STRIP_E_STATE: "call out of order",
+    STRIP_E_KERNEL: "kernel error",
+    STRIP_E_NODEVICE: "no CUDA device",
+}
+
+
+class Geometry(ctypes.Structure):
+    _fields_ = [
+        ("radius", ctypes.c_double),
+        ("scintillator_length", ctypes.c_double),
+        ("n_y_pixels", ctypes.c_int32),
+        ("n_z_pixels", ctypes.c_int32),
+        ("pixel_height", ctypes.c_double),
+        ("pixel_width", ctypes.c_double),
+        ("sigma_z", ctypes.c_double),
+        ("sigma_dl", ctypes.c_double),
+        ("center_y", ctypes.c_double),
+        ("center_z", ctypes.c_double),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("n_events", ctypes.c_int64),
+        ("n_empty", ctypes.c_int64),
+        ("n_overflow", ctypes.c_int64),
+        ("n_tiles_z", ctypes.c_int32),
+        ("n_tiles_y", ctypes.c_int32),
+        ("tile_z", ctypes.c_int32),
+        ("tile_y", ctypes.c_int32),
+        ("halo_z", ctypes.c_int32),
+        ("halo_y", ctypes.c_int32),
+        ("n_work_items", ctypes.c_int32),
+        ("n_subsets", ctypes.c_int32),
+        ("max_box_w", ctypes.c_int32),
+        ("max_box_h", ctypes.c_int32),
+        ("smem_bytes", ctypes.c_int32),
+        ("kernel_launches", ctypes.c_int32),
+        ("last_iterate_ms", ctypes.c_double),
+        ("last_setup_ms", ctypes.c_double),
+        ("last_tile_ms", ctypes.c_double),
+    ]
+
+
+class Ellipse(ctypes.Structure):
+    _fields_ = [
+        ("z", ctypes.c_double),
+        ("y", ctypes.c_double),
+        ("a", ctypes.c_double),
+        ("b", ctypes.c_double),
+        ("angle_deg", ctypes.c_double),
+        ("activity", ctypes.c_double),
+    ]
+
+
+PROGRESS_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p)
+
+_P = ctypes.POINTER
+_f = _P(ctypes.c_float)
+_d = _P(ctypes.c_double)
+_ctx = ctypes.c_void_p
+
+# name -> (restype, argtypes); every symbol include/stripmlem.h declares.
+SIGNATURES = {
+    "strip_ctx_create": (ctypes.c_int, [_P(Geometry), ctypes.c_int, _P(ctypes.c_void_p)]),
+    "strip_ctx_destroy": (ctypes.c_int, [_ctx]),
+    "strip_last_error": (ctypes.c_int, [_ctx, ctypes.c_char_p, ctypes.c_size_t]),
+    "strip_device_name": (ctypes.c_int, [_ctx, ctypes.c_char_p, ctypes.c_size_t]),
+    "strip_set_accumulation": (ctypes.c_int, [_ctx, ctypes.c_int]),
+    "strip_get_stats": (ctypes.c_int, [_ctx, _P(Stats)]),
+    "strip_set_events": (ctypes.c_int, [_ctx, _f, _f, _f, ctypes.c_int64, ctypes.c_int]),
+    "strip_set_responses": (ctypes.c_int, [_ctx, _f, ctypes.c_int64, ctypes.c_int]),
+    "strip_set_events_device": (
+        ctypes.c_int,
+        [_ctx, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int],
+    ),
+    "strip_set_image": (ctypes.c_int, [_ctx, _f]),
+    "strip_get_image": (ctypes.c_int, [_ctx, _f]),
+    "strip_get_sensitivity": (ctypes.c_int, [_ctx, ctypes.c_int, _f]),
+    "strip_iterate": (
+        ctypes.c_int,
+        [_ctx, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, PROGRESS_CB, ctypes.c_void_p],
+    ),
+    "strip_forward": (ctypes.c_int, [_ctx, _f, ctypes.c_double, ctypes.c_double, ctypes.c_int, _d]),
+    "strip_adjoint": (ctypes.c_int, [_ctx, _d, ctypes.c_double, ctypes.c_double, ctypes.c_int, _d]),
+    "strip_grad_sigma": (
+        ctypes.c_int,
+        [_ctx, _f, _d, ctypes.c_double, ctypes.c_double, _d, _d],
+    ),
+    "strip_debug_pixel_sets": (
+        ctypes.c_int,
+        [_ctx, _f, _f, _f, ctypes.c_int64, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_uint64)],
+    ),
+    "strip_probe_fp32_peak": (ctypes.c_int, [ctypes.c_int, _d]),
+    "strip_count_work": (
+        ctypes.c_int,
+        [_ctx, _P(ctypes.c_int64), _P(ctypes.c_int64), _P(ctypes.c_int64)],
+    ),
+    "strip_generate_events": (
+        ctypes.c_int,
+        [_P(Geometry), _P(Ellipse), ctypes.c_int, ctypes.c_uint64, ctypes.c_int64, _f, _f, _f],
+    ),
+}
+
+_lib = None
+
+
+def load():
+    """Loads lib/libstripmlem.so (raises OSError when it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError(
+            f"{LIB_PATH} is missing: build it with `make -C j-pet-mlem-old_b200` "
+            "(there is no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
