@@ -108,7 +108,7 @@ ScannerF make_scanner(const strip_geometry& g) {
   return s;
 }
 
-KernelF make_kernel(double sigma_z, double sigma_dl) {
+KernelF make_kernel(double sigma_z, double sigma_dl, float pw) {
   KernelF k;
   const float sz = (float)sigma_z, sdl = (float)sigma_dl;
   k.ipsz = 1.0f / (sz * sz);
@@ -116,6 +116,10 @@ KernelF make_kernel(double sigma_z, double sigma_dl) {
   k.kc = (float)((1.0 / (2.0 * M_PI * M_PI)) *
                  (double)sqrtf((k.ipsz * k.ipsz) * k.ipsdl));
   k.c1 = -kLog2e * k.ipsz;
+  k.r1 = 2.0f * k.c1 * pw;
+  k.r0 = k.c1 * pw * pw;
+  k.q = (float)exp2(2.0 * (double)k.c1 * (double)pw * (double)pw);
+  k.lg2kc = (float)log2((double)k.kc);
   return k;
 }
 
@@ -138,10 +142,14 @@ Tiling choose_tiling(const strip_ctx* ctx, int max_w, int max_h) {
   Tiling t{};
   int TX = 32, TY = 32;
   int HX = max_w / 2 + 2, HY = max_h / 2 + 2;
+  // per-warp event tables hold a whole event box when it has <= 128 rows
+  t.row_cap = std::min(128, std::max(32, (max_h + 31) / 32 * 32));
   for (;;) {
     const int WX = std::min(n_z, TX + 2 * HX), WY = std::min(n_y, TY + 2 * HY);
     const int WS = WX | 1;
-    const int bytes = 2 * WY * WS * 4;
+    // groups of a block of row_cap rows whose runs fit a window row
+    t.bit_words = (t.row_cap * ((WX + 2) / 3) + 31) / 32 + 1;
+    const int bytes = tile_smem_bytes(WY, WS, t.row_cap, t.bit_words);
     if (bytes <= budget || (HX <= 8 && HY <= 8)) {
       t.TX = TX;
       t.TY = TY;
@@ -251,7 +259,7 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
   const int64_t per_sub = (int64_t)(total / (unsigned long long)n_subsets) + 1;
   const int64_t target = (int64_t)ctx->sm_count * 2 * 8;
   const int64_t chunk =
-      std::min<int64_t>(1 << 15, std::max<int64_t>(64, per_sub / target + 1));
+      std::min<int64_t>(1 << 15, std::max<int64_t>(2048, per_sub / target + 1));
   for (int sb = 0; sb < n_subsets; ++sb) {
     ib[sb] = (int)items.size();
     for (int tile = 0; tile < t.n_tiles; ++tile) {
@@ -354,7 +362,7 @@ int check_ready(strip_ctx* ctx) {
 LaunchArgs base_args(strip_ctx* ctx) {
   LaunchArgs a{};
   a.s = ctx->s;
-  a.k = make_kernel(ctx->g.sigma_z, ctx->g.sigma_dl);
+  a.k = make_kernel(ctx->g.sigma_z, ctx->g.sigma_dl, ctx->s.pw);
   a.t = ctx->t;
   a.zu = ctx->d_zu;
   a.zd = ctx->d_zd;
@@ -363,6 +371,9 @@ LaunchArgs base_args(strip_ctx* ctx) {
   a.rho = ctx->d_rho;
   a.acc = ctx->d_acc;
   a.status = ctx->d_status;
+  // global path: blocks of 32 rows of at most max_w columns
+  a.gcap = 32;
+  a.gbit_words = (32 * ((std::max(ctx->max_w, 1) + 2) / 3) + 31) / 32 + 1;
   return a;
 }
 
@@ -670,7 +681,7 @@ int strip_forward(strip_ctx* ctx, const float* rho, double sigma_z,
   int rc = STRIP_OK;
   if (e == cudaSuccess) {
     LaunchArgs a = base_args(ctx);
-    a.k = make_kernel(sigma_z, sigma_dl);
+    a.k = make_kernel(sigma_z, sigma_dl, ctx->s.pw);
     a.rho = d_img;
     a.sens = (mode == STRIP_MODE_GPU) ? ctx->d_sens5 : nullptr;
     a.y_out = d_y;
@@ -708,7 +719,7 @@ int strip_adjoint(strip_ctx* ctx, const double* w, double sigma_z,
   int rc = STRIP_OK;
   if (e == cudaSuccess) {
     LaunchArgs a = base_args(ctx);
-    a.k = make_kernel(sigma_z, sigma_dl);
+    a.k = make_kernel(sigma_z, sigma_dl, ctx->s.pw);
     a.acc = d_acc;
     a.w_in = d_w;
     rc = run_all(ctx, OP_ADJOINT, mode, a);

@@ -27,7 +27,9 @@ struct WorkItem {
 struct Tiling {
   int TX, TY, HX, HY, ntx, nty, n_tiles;
   int WXmax, WYmax, WS;
-  int smem_bytes;
+  int row_cap;     // rows per per-warp event table (multiple of 32)
+  int bit_words;   // words of the per-warp row-start bitmap
+  int smem_bytes;  // windows + per-warp event tables
 };
 
 __host__ __device__ inline void tile_window(const Tiling& t, int n_z, int n_y,
@@ -71,10 +73,13 @@ struct LaunchArgs {
   const double* w_in;    // OP_ADJOINT / OP_GRAD: per event weights (caller order)
   double* grad_out;      // OP_GRAD: 2 doubles (atomic)
   float sz, sdl;         // OP_GRAD: model sigmas
+  int gcap, gbit_words;  // event tables of the global path
   int* status;           // device status word (0 = ok)
 };
 
 // ---- launchers (strip_kernels.cu) ----------------------------------------
+int tile_smem_bytes(int WYmax, int WS, int row_cap, int bit_words);
+int global_smem_bytes(int cap, int bit_words);
 cudaError_t launch_event_boxes(const ScannerF& s, const float* zu,
                                const float* zd, const float* dl, int64_t n,
                                int4* boxes, int* max_wh, unsigned long long* n_empty,

@@ -25,6 +25,11 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
+__device__ __forceinline__ float lg2_approx(float x) {
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ float rcp_approx(float x) {
   float y;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -37,7 +42,12 @@ constexpr float kLog2e = 1.4426950408889634f;
 // from the geometry's sigmas that fix the pixel sets).
 struct KernelF {
   float ipsz, ipsdl, kc;
-  float c1;  // -log2(e) * ipsz
+  float c1;      // -log2(e) * ipsz
+  // Gaussian recurrence along a row of pixel pitch pw, t -> t + pw:
+  //   E(t + pw) = E(t) * R(t),  R(t) = 2^(r1 t + r0),  R(t + pw) = R(t) * q
+  float r1, r0;  // 2 c1 pw, c1 pw^2
+  float q;       // 2^(2 c1 pw^2)
+  float lg2kc;   // log2(kc)
 };
 
 // GaussianKernel, one row.
@@ -89,7 +99,9 @@ struct AnalyticRow {
     dytan = dy * tan;
   }
   __device__ __forceinline__ float eval(const KernelF& k, float dz) const {
-    const float t = dz - dytan;
+    return eval_t(k, dz - dytan);
+  }
+  __device__ __forceinline__ float eval_t(const KernelF& k, float t) const {
     const float norm = fmaf(n1, t, n0);
     const float bia = fmaf(u1, t, u0);
     const float bib = fmaf(2.0f * k.ipsz, t * t, cr);

@@ -4,13 +4,18 @@
 //       into image tiles (events are iteration-invariant, so this is paid once)
 //   k_tile      the hot kernel: one CTA per (tile, event chunk) work item.  The
 //       tile's window of the image (tile + halo) is staged in shared memory
-//       together with a shared-memory backprojection accumulator; a warp takes
-//       one event at a time: (a) scans the event's clamped bounding box with the
-//       exact binary32 ellipse test and evaluates the TOF kernel, (b) sums
-//       K * rho (* s) into the per-event normalisation D_e (compensated or
-//       binary64 per lane, binary64 across lanes), (c) scatters K / D_e into
-//       the shared accumulator with shared-memory atomics, and finally flushes
-//       the window to the global binary64 accumulator.
+//       next to a shared-memory backprojection accumulator.  A warp takes one
+//       event at a time:
+//         (a) event setup and the exact per-row pixel runs of its 3-sigma
+//             ellipse (strip_rows.cuh), the TOF kernel's row constants;
+//         (b) D_e = sum K * rho (* s): lane per row, the Gaussian advanced
+//             along the row's run by the recurrence E <- E * R, R <- R * q
+//             (two multiplies per pixel), per-row binary32 partials combined
+//             across rows in binary32, Kahan or binary64, and across lanes in
+//             binary64;
+//         (c) the same walk scatters K / D_e with shared-memory atomics;
+//       and the window is finally flushed into the global binary64
+//       accumulator.
 //   k_global    the same per-event work for events whose box does not fit a
 //       window (global loads, global binary64 atomics).
 //   k_update    (d) rho_j <- rho_j * acc_j * scale, acc_j <- 0.
@@ -19,6 +24,7 @@
 // 220-298) and the warp kernel (src/2d/strip/cuda/reconstruction/
 // warp_granularity.cuh:20-176).
 #include "strip_internal.h"
+#include "strip_rows.cuh"
 
 namespace stripmlem {
 
@@ -26,6 +32,7 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -49,17 +56,17 @@ __device__ __forceinline__ EventF shfl_event(const EventF& m, int src) {
   return e;
 }
 
-// Per-lane accumulation of the normalisation sum.
+// Accumulation of the per-row partial sums of D_e within a lane.
 template <int ACC>
-struct Accum;
+struct RowSum;
 template <>
-struct Accum<STRIP_ACCUM_FP32> {
+struct RowSum<STRIP_ACCUM_FP32> {
   float s = 0.0f;
   __device__ __forceinline__ void add(float x) { s += x; }
   __device__ __forceinline__ double total() const { return (double)s; }
 };
 template <>
-struct Accum<STRIP_ACCUM_KAHAN> {
+struct RowSum<STRIP_ACCUM_KAHAN> {
   float s = 0.0f, c = 0.0f;
   __device__ __forceinline__ void add(float x) {
     const float yv = __fsub_rn(x, c);
@@ -72,21 +79,10 @@ struct Accum<STRIP_ACCUM_KAHAN> {
   }
 };
 template <>
-struct Accum<STRIP_ACCUM_FP64> {
+struct RowSum<STRIP_ACCUM_FP64> {
   double s = 0.0;
   __device__ __forceinline__ void add(float x) { s += (double)x; }
   __device__ __forceinline__ double total() const { return s; }
-};
-
-template <int MODE>
-struct RowEvalT;
-template <>
-struct RowEvalT<STRIP_MODE_CPU> {
-  using T = GaussRow;
-};
-template <>
-struct RowEvalT<STRIP_MODE_GPU> {
-  using T = AnalyticRow;
 };
 
 // Shared-memory window of the image: w = rho (* s), acc = partial backprojection.
@@ -94,11 +90,12 @@ struct SmemWin {
   const float* w;
   float* acc;
   int wx0, wy0, WS;
-  __device__ __forceinline__ float read(int ix, int iy) const {
-    return w[(iy - wy0) * WS + (ix - wx0)];
+  __device__ __forceinline__ int ptr(int iy, int col) const {
+    return (iy - wy0) * WS + (col - wx0);
   }
-  __device__ __forceinline__ void add(int ix, int iy, float v) const {
-    atomicAdd(acc + (iy - wy0) * WS + (ix - wx0), v);
+  __device__ __forceinline__ float read(int p, int j) const { return w[p + j]; }
+  __device__ __forceinline__ void add(int p, int j, float v) const {
+    atomicAdd(acc + p + j, v);
   }
 };
 
@@ -109,74 +106,183 @@ struct GlobalWin {
   const float* sens;
   double* acc;
   int n_z;
-  __device__ __forceinline__ float read(int ix, int iy) const {
-    const int64_t gi = (int64_t)iy * n_z + ix;
-    float v = __ldg(rho + gi);
-    if (MODE == STRIP_MODE_GPU) v *= __ldg(sens + gi);
+  __device__ __forceinline__ int64_t ptr(int iy, int col) const {
+    return (int64_t)iy * n_z + col;
+  }
+  __device__ __forceinline__ float read(int64_t p, int j) const {
+    float v = __ldg(rho + p + j);
+    if (MODE == STRIP_MODE_GPU) v *= __ldg(sens + p + j);
     return v;
   }
-  __device__ __forceinline__ void add(int ix, int iy, float v) const {
-    atomicAdd(acc + (int64_t)iy * n_z + ix, (double)v);
+  __device__ __forceinline__ void add(int64_t p, int j, float v) const {
+    atomicAdd(acc + p + j, (double)v);
   }
 };
 
-// Row constants of 32 consecutive rows, one per lane, broadcast by shuffles.
+// Walks the lane's share of the flattened pixel list of rows
+// [row0, row0 + nrows).  For each run piece, f(r, col, cnt) is called with
+// the row index within the block, the first column and the pixel count.
+template <class F>
+__device__ __forceinline__ void walk_share(const RowTables& T, int nrows,
+                                           int n, int lane, F&& f) {
+  int f0, f1;
+  int r = lane_share(T, nrows, n, lane, f0, f1);
+  int pos = f0;
+  while (pos < f1) {
+    const int rs = T.start[r], re = T.start[r + 1];
+    if (re > pos) {
+      const int cnt = min(re, f1) - pos;
+      f(r, T.lo[r] + (pos - rs), cnt);
+      pos += cnt;
+    }
+    ++r;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Lane-per-row event processing.  The box rows of an event are ranked
+// middle-out (the centre row first, then alternately below and above), so a
+// block of 32 consecutive ranks holds rows of similar run length; lane l of
+// block k owns the row of rank 32k + l.  A lane keeps its rows' run (lo, len)
+// and recurrence state (E0, R0, pref) in registers across both passes: pass 1
+// walks its runs with E <- E*R, R <- R*q (no per-pixel exponential, no
+// per-pixel bookkeeping), pass 2 walks them again from the stored state.
+// Events with more than kRowBlocks*32 rows are processed in super-blocks and
+// rebuilt for pass 2.
+// ---------------------------------------------------------------------------
+constexpr int kRowBlocks = 4;
+
+__device__ __forceinline__ int ranked_row(int H, int i) {
+  const int mid = (H - 1) >> 1;
+  return mid + ((i & 1) ? ((i + 1) >> 1) : -(i >> 1));
+}
+
 template <int MODE>
-struct RowPack {
-  RowSet rs;
-  typename RowEvalT<MODE>::T re;
+struct LaneRows;
+
+// GaussianKernel: K = pref * E along the run, E(t0) = 2^(c1 t0^2 + c0)
+template <>
+struct LaneRows<STRIP_MODE_CPU> {
+  int iy[kRowBlocks], lo[kRowBlocks], len[kRowBlocks];
+  float E0[kRowBlocks], R0[kRowBlocks], pref[kRowBlocks];
+};
+// AnalyticKernel: direct evaluation per pixel from the row constants
+template <>
+struct LaneRows<STRIP_MODE_GPU> {
+  int iy[kRowBlocks], lo[kRowBlocks], len[kRowBlocks];
+  float t0[kRowBlocks], n0[kRowBlocks], n1[kRowBlocks], u0[kRowBlocks],
+      u1[kRowBlocks], cr[kRowBlocks];
 };
 
+// Builds the lane's rows of ranks [rank0, rank0 + 32*kRowBlocks).
 template <int MODE>
-__device__ __forceinline__ RowPack<MODE> shfl_row(const RowPack<MODE>& m,
-                                                  int src) {
-  RowPack<MODE> r;
-  r.rs.dy = __shfl_sync(kFull, m.rs.dy, src);
-  r.rs.Ady2 = __shfl_sync(kFull, m.rs.Ady2, src);
-  r.rs.Bdy = __shfl_sync(kFull, m.rs.Bdy, src);
-  r.re.pref = __shfl_sync(kFull, m.re.pref, src);
-  r.re.c0 = __shfl_sync(kFull, m.re.c0, src);
-  r.re.dytan = __shfl_sync(kFull, m.re.dytan, src);
-  return r;
-}
-template <>
-__device__ __forceinline__ RowPack<STRIP_MODE_GPU> shfl_row(
-    const RowPack<STRIP_MODE_GPU>& m, int src) {
-  RowPack<STRIP_MODE_GPU> r;
-  r.rs.dy = __shfl_sync(kFull, m.rs.dy, src);
-  r.rs.Ady2 = __shfl_sync(kFull, m.rs.Ady2, src);
-  r.rs.Bdy = __shfl_sync(kFull, m.rs.Bdy, src);
-  r.re.n0 = __shfl_sync(kFull, m.re.n0, src);
-  r.re.n1 = __shfl_sync(kFull, m.re.n1, src);
-  r.re.u0 = __shfl_sync(kFull, m.re.u0, src);
-  r.re.u1 = __shfl_sync(kFull, m.re.u1, src);
-  r.re.cr = __shfl_sync(kFull, m.re.cr, src);
-  r.re.dytan = __shfl_sync(kFull, m.re.dytan, src);
-  return r;
+__device__ __forceinline__ void build_lane_rows(const ScannerF& s,
+                                                const KernelF& k,
+                                                const EventF& e,
+                                                const EventRows& er, int H,
+                                                int rank0, int lane,
+                                                LaneRows<MODE>& L) {
+#pragma unroll
+  for (int b = 0; b < kRowBlocks; ++b) {
+    L.len[b] = 0;
+    const int i = rank0 + 32 * b + lane;
+    if (i < H) {
+      const int iy = e.tly + ranked_row(H, i);
+      const RowSet rs = row_set(s, e, iy);
+      int lo;
+      const int len = row_run(s, e, er, rs, lo);
+      L.iy[b] = iy;
+      L.lo[b] = lo;
+      L.len[b] = len;
+      if (len > 0) {
+        const float t0 = (fmaf((float)lo, s.pw, s.tl_z_half_w) - e.z);
+        if constexpr (MODE == STRIP_MODE_CPU) {
+          GaussRow g;
+          g.init(k, s.R, e.y, e.tan, e.sec, rs.dy);
+          const float t = t0 - g.dytan;
+          L.E0[b] = ex2_approx(fmaf(k.c1 * t, t, g.c0));
+          L.R0[b] = ex2_approx(fmaf(k.r1, t, k.r0));
+          L.pref[b] = g.pref;
+        } else {
+          AnalyticRow g;
+          g.init(k, s.R, e.y, e.tan, e.sec, rs.dy);
+          L.t0[b] = t0 - g.dytan;
+          L.n0[b] = g.n0;
+          L.n1[b] = g.n1;
+          L.u0[b] = g.u0;
+          L.u1[b] = g.u1;
+          L.cr[b] = g.cr;
+        }
+      }
+    }
+  }
 }
 
-// Visits every in-ellipse pixel of event e: rows are taken 32 at a time (one
-// row's constants per lane), then the warp sweeps each row's bbox columns
-// with lanes side by side.  f(ix, iy, K) is called for in-ellipse pixels.
-template <int MODE, class F>
-__device__ __forceinline__ void for_each_pixel(const ScannerF& s,
-                                               const KernelF& k,
-                                               const EventF& e, int lane,
-                                               F&& f) {
-  for (int rb = e.tly; rb < e.bry; rb += 32) {
-    RowPack<MODE> mine = {};
-    const int my_row = rb + lane;
-    if (my_row < e.bry) {
-      mine.rs = row_set(s, e, my_row);
-      mine.re.init(k, s.R, e.y, e.tan, e.sec, mine.rs.dy);
+// Pass 1 over the lane's rows: sum over runs of K_j * w_j.
+template <int MODE, int ACC, class Win>
+__device__ __forceinline__ void pass1_rows(const ScannerF& s, const KernelF& k,
+                                           const LaneRows<MODE>& L, int nb,
+                                           const Win& win, RowSum<ACC>& acc) {
+#pragma unroll
+  for (int b = 0; b < kRowBlocks; ++b) {
+    if (b < nb && L.len[b] > 0) {
+      const auto p = win.ptr(L.iy[b], L.lo[b]);
+      const int n = L.len[b];
+      float a = 0.0f;
+      if constexpr (MODE == STRIP_MODE_CPU) {
+        float E = L.E0[b], R = L.R0[b];
+#pragma unroll 4
+        for (int j = 0; j < n; ++j) {
+          a = fmaf(E, win.read(p, j), a);
+          E *= R;
+          R *= k.q;
+        }
+        acc.add(L.pref[b] * a);
+      } else {
+        AnalyticRow g;
+        g.n0 = L.n0[b];
+        g.n1 = L.n1[b];
+        g.u0 = L.u0[b];
+        g.u1 = L.u1[b];
+        g.cr = L.cr[b];
+#pragma unroll 2
+        for (int j = 0; j < n; ++j)
+          a = fmaf(g.eval_t(k, fmaf((float)j, s.pw, L.t0[b])), win.read(p, j), a);
+        acc.add(a);
+      }
     }
-    const int nr = min(32, e.bry - rb);
-    for (int j = 0; j < nr; ++j) {
-      const RowPack<MODE> r = shfl_row<MODE>(mine, j);
-      const int iy = rb + j;
-      for (int iz = e.tlx + lane; iz < e.brx; iz += 32) {
-        const float dz = col_dz(s, e, iz);
-        if (in_ellipse(r.rs, e.C, dz)) f(iz, iy, r.re.eval(k, dz));
+  }
+}
+
+// Pass 2 over the lane's rows: acc_j += K_j * scale.
+template <int MODE, class Win>
+__device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
+                                           const LaneRows<MODE>& L, int nb,
+                                           const Win& win, float scale) {
+#pragma unroll
+  for (int b = 0; b < kRowBlocks; ++b) {
+    if (b < nb && L.len[b] > 0) {
+      const auto p = win.ptr(L.iy[b], L.lo[b]);
+      const int n = L.len[b];
+      if constexpr (MODE == STRIP_MODE_CPU) {
+        float E = L.E0[b], R = L.R0[b];
+        const float sc = L.pref[b] * scale;
+#pragma unroll 4
+        for (int j = 0; j < n; ++j) {
+          win.add(p, j, E * sc);
+          E *= R;
+          R *= k.q;
+        }
+      } else {
+        AnalyticRow g;
+        g.n0 = L.n0[b];
+        g.n1 = L.n1[b];
+        g.u0 = L.u0[b];
+        g.u1 = L.u1[b];
+        g.cr = L.cr[b];
+#pragma unroll 2
+        for (int j = 0; j < n; ++j)
+          win.add(p, j, g.eval_t(k, fmaf((float)j, s.pw, L.t0[b])) * scale);
       }
     }
   }
@@ -186,11 +292,18 @@ template <int OP, int MODE, int ACC, class Win>
 __device__ __forceinline__ void process_event(const LaunchArgs& a,
                                               const EventF& e, const Win& win,
                                               int lane, int64_t pos) {
+  const int H = e.bry - e.tly;
+  if (H <= 0 || e.brx <= e.tlx) return;
+  const EventRows er = event_rows(a.s, e);
+  constexpr int kSuper = 32 * kRowBlocks;
+  LaneRows<MODE> L;
+  float scale;
   if (OP == OP_MLEM || OP == OP_FORWARD) {
-    Accum<ACC> acc;
-    for_each_pixel<MODE>(a.s, a.k, e, lane, [&](int ix, int iy, float kv) {
-      acc.add(kv * win.read(ix, iy));
-    });
+    RowSum<ACC> acc;
+    for (int r0 = 0; r0 < H; r0 += kSuper) {
+      build_lane_rows<MODE>(a.s, a.k, e, er, H, r0, lane, L);
+      pass1_rows<MODE, ACC>(a.s, a.k, L, min(kRowBlocks, (H - r0 + 31) >> 5), win, acc);
+    }
     const double D = warp_sum(acc.total());
     if (OP == OP_FORWARD) {
       if (lane == 0) a.y_out[a.perm[pos]] = D;
@@ -198,28 +311,37 @@ __device__ __forceinline__ void process_event(const LaunchArgs& a,
     }
     // reconstruction.h:290 -- an all-zero denominator contributes nothing
     if (!(D > 0.0)) return;
-    const float inv = (float)(1.0 / D);
-    for_each_pixel<MODE>(a.s, a.k, e, lane, [&](int ix, int iy, float kv) {
-      win.add(ix, iy, kv * inv);
-    });
-  } else if (OP == OP_ADJOINT) {
-    const float w = (float)a.w_in[a.perm[pos]];
-    if (w == 0.0f) return;
-    for_each_pixel<MODE>(a.s, a.k, e, lane, [&](int ix, int iy, float kv) {
-      win.add(ix, iy, kv * w);
-    });
+    scale = (float)(1.0 / D);
+  } else {
+    scale = (float)a.w_in[a.perm[pos]];
+    if (scale == 0.0f) return;
+  }
+  if ((OP == OP_MLEM) && H <= kSuper) {
+    pass2_rows<MODE>(a.s, a.k, L, (H + 31) >> 5, win, scale);
+    return;
+  }
+  for (int r0 = 0; r0 < H; r0 += kSuper) {
+    build_lane_rows<MODE>(a.s, a.k, e, er, H, r0, lane, L);
+    pass2_rows<MODE>(a.s, a.k, L, min(kRowBlocks, (H - r0 + 31) >> 5), win, scale);
   }
 }
 
+__device__ __forceinline__ RowTables warp_tables(char* base, int cap, int warp) {
+  return row_tables_at(base + (size_t)warp * row_table_bytes(cap), cap);
+}
+
 template <int OP, int MODE, int ACC>
-__global__ void __launch_bounds__(kThreads) k_tile(LaunchArgs a) {
-  extern __shared__ float smem[];
+__global__ void __launch_bounds__(kThreads, 2) k_tile(LaunchArgs a) {
+  extern __shared__ __align__(16) char smem_raw[];
   const WorkItem it = a.items[blockIdx.x];
   int wx0, wy0, wx1, wy1;
   tile_window(a.t, a.s.n_z, a.s.n_y, it.tile, wx0, wy0, wx1, wy1);
   const int wxn = wx1 - wx0, wyn = wy1 - wy0, WS = a.t.WS;
-  float* s_w = smem;
-  float* s_acc = smem + a.t.WYmax * WS;
+  float* s_w = reinterpret_cast<float*>(smem_raw);
+  float* s_acc = s_w + a.t.WYmax * WS;
+  __shared__ int s_next_group;
+  if (threadIdx.x == 0) s_next_group = 0;
+  const int lane = threadIdx.x & 31;
   constexpr bool kReads = (OP == OP_MLEM || OP == OP_FORWARD);
   constexpr bool kWrites = (OP == OP_MLEM || OP == OP_ADJOINT);
   for (int q = threadIdx.x; q < wxn * wyn; q += blockDim.x) {
@@ -234,11 +356,14 @@ __global__ void __launch_bounds__(kThreads) k_tile(LaunchArgs a) {
   }
   __syncthreads();
   const SmemWin win{s_w, s_acc, wx0, wy0, WS};
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nw = blockDim.x >> 5;
   const int64_t end = it.begin + it.count;
-  for (int64_t base = it.begin + (int64_t)warp * 32; base < end;
-       base += (int64_t)nw * 32) {
+  // warps pull groups of 32 events from a shared counter until the item is done
+  for (;;) {
+    int g = 0;
+    if (lane == 0) g = atomicAdd(&s_next_group, 1);
+    g = __shfl_sync(kFull, g, 0);
+    const int64_t base = it.begin + (int64_t)g * 32;
+    if (base >= end) break;
     const int64_t ei = base + lane;
     EventF mine = {};
     if (ei < end) event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], mine);
@@ -406,64 +531,60 @@ __global__ void k_sensitivity(ScannerF s, int five_point, float* out) {
   }
 }
 
-// Pixel-set parity: one warp per event, the same enumeration as k_tile.
-__global__ void k_debug_sets(ScannerF s, const float* zu, const float* zd,
-                             const float* dl, int64_t n, int32_t* n_bb,
-                             int32_t* n_in, uint64_t* digest) {
-  const int lane = threadIdx.x & 31;
+// Pixel-set parity and work counts: one warp per event, the same row-run
+// enumeration (build_rows / walk_share) as the reconstruction kernels.
+template <bool DEBUG>
+__global__ void __launch_bounds__(kThreads) k_sets(
+    ScannerF s, const float* zu, const float* zd, const float* dl, int64_t n,
+    int cap, int32_t* n_bb, int32_t* n_in, uint64_t* digest,
+    unsigned long long* totals) {
+  extern __shared__ __align__(16) char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const RowTables T = warp_tables(smem_raw, cap, warp);
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwt = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  KernelF k{s.ipsz, s.ipsdl, s.kc, -kLog2e * s.ipsz};
+  const KernelF k{};
+  unsigned long long tb = 0, ti = 0, tn = 0;
   for (int64_t i = wid; i < n; i += nwt) {
     EventF e;
     event_setup(s, zu[i], zd[i], dl[i], e);
+    const int H = e.bry - e.tly, W = e.brx - e.tlx;
     unsigned cnt = 0;
     unsigned long long h = 0;
-    for_each_pixel<STRIP_MODE_CPU>(s, k, e, lane, [&](int ix, int iy, float) {
-      ++cnt;
-      h += mix64((uint64_t)((int64_t)iy * s.n_z + ix) + 1u);
-    });
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      cnt += __shfl_xor_sync(kFull, cnt, o);
-      h += __shfl_xor_sync(kFull, h, o);
+    if (H > 0 && W > 0) {
+      const EventRows er = event_rows(s, e);
+      for (int r0 = 0; r0 < H; r0 += cap) {
+        const int nr = min(cap, H - r0);
+        if (r0 > 0) __syncwarp();
+        const int m = build_rows<0>(s, k, e, er, e.tly + r0, nr, T, lane);
+        cnt += m;
+        if (DEBUG) {
+          walk_share(T, nr, m, lane, [&](int r, int col, int c) {
+            const int64_t idx = (int64_t)(e.tly + r0 + r) * s.n_z + col;
+            for (int j = 0; j < c; ++j) h += mix64((uint64_t)(idx + j) + 1u);
+          });
+        }
+      }
+      __syncwarp();
     }
-    if (lane == 0) {
-      const int w = e.brx - e.tlx, hh = e.bry - e.tly;
-      if (n_bb) n_bb[i] = (w > 0 && hh > 0) ? w * hh : 0;
-      if (n_in) n_in[i] = (int32_t)cnt;
-      if (digest) digest[i] = h;
+    if (DEBUG) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(kFull, h, o);
+      if (lane == 0) {
+        if (n_bb) n_bb[i] = (H > 0 && W > 0) ? W * H : 0;
+        if (n_in) n_in[i] = (int32_t)cnt;
+        if (digest) digest[i] = h;
+      }
+    } else if (lane == 0 && H > 0 && W > 0) {
+      tb += (unsigned long long)W * H;
+      ti += cnt;
+      tn += cnt > 0;
     }
   }
-}
-
-// Work totals over binned events (same enumeration as k_tile).
-__global__ void k_count_work(ScannerF s, const float* zu, const float* zd,
-                             const float* dl, int64_t n,
-                             unsigned long long* out) {
-  const int lane = threadIdx.x & 31;
-  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwt = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  KernelF k{s.ipsz, s.ipsdl, s.kc, -kLog2e * s.ipsz};
-  unsigned long long bb = 0, in = 0, ne = 0;
-  for (int64_t i = wid; i < n; i += nwt) {
-    EventF e;
-    event_setup(s, zu[i], zd[i], dl[i], e);
-    unsigned cnt = 0;
-    for_each_pixel<STRIP_MODE_CPU>(s, k, e, lane,
-                                   [&](int, int, float) { ++cnt; });
-    const int w = e.brx - e.tlx, h = e.bry - e.tly;
-    if (lane == 0 && w > 0 && h > 0) bb += (unsigned long long)w * h;
-    in += cnt;
-    const unsigned tot = __reduce_add_sync(kFull, cnt);
-    if (lane == 0 && tot > 0) ++ne;
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) in += __shfl_xor_sync(kFull, in, o);
-  if (lane == 0) {
-    atomicAdd(out, bb);
-    atomicAdd(out + 1, in);
-    atomicAdd(out + 2, ne);
+  if (!DEBUG && lane == 0) {
+    atomicAdd(totals, tb);
+    atomicAdd(totals + 1, ti);
+    atomicAdd(totals + 2, tn);
   }
 }
 
@@ -501,6 +622,8 @@ int grid_for(int64_t n, int per_block = kThreads, int cap = 148 * 16) {
   return (int)g;
 }
 
+constexpr int kSetsCap = 64;
+
 template <int OP, int MODE, int ACC>
 cudaError_t launch_tile_t(const LaunchArgs& a, cudaStream_t st) {
   auto fn = k_tile<OP, MODE, ACC>;
@@ -513,7 +636,7 @@ cudaError_t launch_tile_t(const LaunchArgs& a, cudaStream_t st) {
 
 template <int OP, int MODE, int ACC>
 cudaError_t launch_global_t(const LaunchArgs& a, cudaStream_t st) {
-  const int grid = grid_for(a.g_count, 8 * 32);
+  const int grid = grid_for(a.g_count, kWarps * 32);
   k_global<OP, MODE, ACC><<<grid, kThreads, 0, st>>>(a);
   return cudaGetLastError();
 }
@@ -535,6 +658,18 @@ cudaError_t launch_global_t(const LaunchArgs& a, cudaStream_t st) {
       return FN<op, STRIP_MODE_GPU, STRIP_ACCUM_FP64>(a, st);              \
     return FN<op, STRIP_MODE_GPU, STRIP_ACCUM_KAHAN>(a, st);               \
   } while (0)
+
+int tile_smem_bytes(int WYmax, int WS, int row_cap, int bit_words) {
+  (void)row_cap;
+  (void)bit_words;
+  return 2 * WYmax * WS * 4;
+}
+
+int global_smem_bytes(int cap, int bit_words) {
+  (void)cap;
+  (void)bit_words;
+  return 0;
+}
 
 cudaError_t launch_tile(int op, int mode, int accum, const LaunchArgs& a,
                         cudaStream_t st) {
@@ -615,14 +750,9 @@ cudaError_t launch_debug_sets(const ScannerF& s, const float* zu,
                               int32_t* n_bb, int32_t* n_in, uint64_t* digest,
                               cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  k_debug_sets<<<grid_for(n * 32), kThreads, 0, st>>>(s, zu, zd, dl, n, n_bb,
-                                                      n_in, digest);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_scale_copy(const double* acc, const float* sens,
-                              double* out, int64_t n_pix, cudaStream_t st) {
-  k_scale_copy<<<grid_for(n_pix), kThreads, 0, st>>>(acc, sens, out, n_pix);
+  const int smem = kWarps * row_table_bytes(kSetsCap);
+  k_sets<true><<<grid_for(n * 32), kThreads, smem, st>>>(
+      s, zu, zd, dl, n, kSetsCap, n_bb, n_in, digest, nullptr);
   return cudaGetLastError();
 }
 
@@ -630,7 +760,15 @@ cudaError_t launch_count_work(const ScannerF& s, const float* zu,
                               const float* zd, const float* dl, int64_t n,
                               unsigned long long* out, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  k_count_work<<<grid_for(n * 32), kThreads, 0, st>>>(s, zu, zd, dl, n, out);
+  const int smem = kWarps * row_table_bytes(kSetsCap);
+  k_sets<false><<<grid_for(n * 32), kThreads, smem, st>>>(
+      s, zu, zd, dl, n, kSetsCap, nullptr, nullptr, nullptr, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scale_copy(const double* acc, const float* sens,
+                              double* out, int64_t n_pix, cudaStream_t st) {
+  k_scale_copy<<<grid_for(n_pix), kThreads, 0, st>>>(acc, sens, out, n_pix);
   return cudaGetLastError();
 }
 
