@@ -105,6 +105,8 @@ ScannerF make_scanner(const strip_geometry& g) {
   s.ipsdl = 1.0f / (s.sdl * s.sdl);
   s.kc = (float)((1.0 / (2.0 * M_PI * M_PI)) *
                  (double)sqrtf((s.ipsz * s.ipsz) * s.ipsdl));
+  s.inv_pw = 1.0f / s.pw;
+  s.inv2z = 0.5f / s.ipsz;
   return s;
 }
 

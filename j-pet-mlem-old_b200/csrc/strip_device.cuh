@@ -20,6 +20,9 @@ struct ScannerF {
   float tl_y, tl_z, tl_y_half_h, tl_z_half_w, half_L;
   float ipsz, ipsdl, kc;
   int n_y, n_z;  // after narrowing to int16, as Scanner<float, short>
+  // launch constants of the closed-form row runs (not part of the exact
+  // set arithmetic): 1 / pw and sigma_z^2 / 2
+  float inv_pw, inv2z;
 };
 
 // One event after Response::calculate_tan_y_z (response.h:22-37) and

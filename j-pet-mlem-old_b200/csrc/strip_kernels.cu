@@ -31,7 +31,8 @@ namespace stripmlem {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;
+constexpr int kGrab = 8;  // events a warp takes from the item per counter step
 constexpr int kWarps = kThreads / 32;
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -150,7 +151,7 @@ __device__ __forceinline__ void walk_share(const RowTables& T, int nrows,
 // Events with more than kRowBlocks*32 rows are processed in super-blocks and
 // rebuilt for pass 2.
 // ---------------------------------------------------------------------------
-constexpr int kRowBlocks = 4;
+constexpr int kRowBlocks = 3;
 
 __device__ __forceinline__ int ranked_row(int H, int i) {
   const int mid = (H - 1) >> 1;
@@ -160,16 +161,20 @@ __device__ __forceinline__ int ranked_row(int H, int i) {
 template <int MODE>
 struct LaneRows;
 
+// Run of block b: lolen[b] = lo << 16 | len (len == 0: no run).
+__device__ __forceinline__ int run_lo(int v) { return v >> 16; }
+__device__ __forceinline__ int run_len(int v) { return v & 0xFFFF; }
+
 // GaussianKernel: K = pref * E along the run, E(t0) = 2^(c1 t0^2 + c0)
 template <>
 struct LaneRows<STRIP_MODE_CPU> {
-  int iy[kRowBlocks], lo[kRowBlocks], len[kRowBlocks];
+  int lolen[kRowBlocks];
   float E0[kRowBlocks], R0[kRowBlocks], pref[kRowBlocks];
 };
 // AnalyticKernel: direct evaluation per pixel from the row constants
 template <>
 struct LaneRows<STRIP_MODE_GPU> {
-  int iy[kRowBlocks], lo[kRowBlocks], len[kRowBlocks];
+  int lolen[kRowBlocks];
   float t0[kRowBlocks], n0[kRowBlocks], n1[kRowBlocks], u0[kRowBlocks],
       u1[kRowBlocks], cr[kRowBlocks];
 };
@@ -184,16 +189,14 @@ __device__ __forceinline__ void build_lane_rows(const ScannerF& s,
                                                 LaneRows<MODE>& L) {
 #pragma unroll
   for (int b = 0; b < kRowBlocks; ++b) {
-    L.len[b] = 0;
+    L.lolen[b] = 0;
     const int i = rank0 + 32 * b + lane;
     if (i < H) {
       const int iy = e.tly + ranked_row(H, i);
       const RowSet rs = row_set(s, e, iy);
       int lo;
       const int len = row_run(s, e, er, rs, lo);
-      L.iy[b] = iy;
-      L.lo[b] = lo;
-      L.len[b] = len;
+      L.lolen[b] = (lo << 16) | len;
       if (len > 0) {
         const float t0 = (fmaf((float)lo, s.pw, s.tl_z_half_w) - e.z);
         if constexpr (MODE == STRIP_MODE_CPU) {
@@ -221,13 +224,16 @@ __device__ __forceinline__ void build_lane_rows(const ScannerF& s,
 // Pass 1 over the lane's rows: sum over runs of K_j * w_j.
 template <int MODE, int ACC, class Win>
 __device__ __forceinline__ void pass1_rows(const ScannerF& s, const KernelF& k,
-                                           const LaneRows<MODE>& L, int nb,
-                                           const Win& win, RowSum<ACC>& acc) {
+                                           const EventF& e, int H, int rank0,
+                                           int lane, const LaneRows<MODE>& L,
+                                           int nb, const Win& win,
+                                           RowSum<ACC>& acc) {
 #pragma unroll
   for (int b = 0; b < kRowBlocks; ++b) {
-    if (b < nb && L.len[b] > 0) {
-      const auto p = win.ptr(L.iy[b], L.lo[b]);
-      const int n = L.len[b];
+    const int n = run_len(L.lolen[b]);
+    if (b < nb && n > 0) {
+      const auto p = win.ptr(e.tly + ranked_row(H, rank0 + 32 * b + lane),
+                             run_lo(L.lolen[b]));
       float a = 0.0f;
       if constexpr (MODE == STRIP_MODE_CPU) {
         float E = L.E0[b], R = L.R0[b];
@@ -257,13 +263,16 @@ __device__ __forceinline__ void pass1_rows(const ScannerF& s, const KernelF& k,
 // Pass 2 over the lane's rows: acc_j += K_j * scale.
 template <int MODE, class Win>
 __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
-                                           const LaneRows<MODE>& L, int nb,
-                                           const Win& win, float scale) {
+                                           const EventF& e, int H, int rank0,
+                                           int lane, const LaneRows<MODE>& L,
+                                           int nb, const Win& win,
+                                           float scale) {
 #pragma unroll
   for (int b = 0; b < kRowBlocks; ++b) {
-    if (b < nb && L.len[b] > 0) {
-      const auto p = win.ptr(L.iy[b], L.lo[b]);
-      const int n = L.len[b];
+    const int n = run_len(L.lolen[b]);
+    if (b < nb && n > 0) {
+      const auto p = win.ptr(e.tly + ranked_row(H, rank0 + 32 * b + lane),
+                             run_lo(L.lolen[b]));
       if constexpr (MODE == STRIP_MODE_CPU) {
         float E = L.E0[b], R = L.R0[b];
         const float sc = L.pref[b] * scale;
@@ -302,7 +311,8 @@ __device__ __forceinline__ void process_event(const LaunchArgs& a,
     RowSum<ACC> acc;
     for (int r0 = 0; r0 < H; r0 += kSuper) {
       build_lane_rows<MODE>(a.s, a.k, e, er, H, r0, lane, L);
-      pass1_rows<MODE, ACC>(a.s, a.k, L, min(kRowBlocks, (H - r0 + 31) >> 5), win, acc);
+      pass1_rows<MODE, ACC>(a.s, a.k, e, H, r0, lane, L,
+                            min(kRowBlocks, (H - r0 + 31) >> 5), win, acc);
     }
     const double D = warp_sum(acc.total());
     if (OP == OP_FORWARD) {
@@ -317,12 +327,13 @@ __device__ __forceinline__ void process_event(const LaunchArgs& a,
     if (scale == 0.0f) return;
   }
   if ((OP == OP_MLEM) && H <= kSuper) {
-    pass2_rows<MODE>(a.s, a.k, L, (H + 31) >> 5, win, scale);
+    pass2_rows<MODE>(a.s, a.k, e, H, 0, lane, L, (H + 31) >> 5, win, scale);
     return;
   }
   for (int r0 = 0; r0 < H; r0 += kSuper) {
     build_lane_rows<MODE>(a.s, a.k, e, er, H, r0, lane, L);
-    pass2_rows<MODE>(a.s, a.k, L, min(kRowBlocks, (H - r0 + 31) >> 5), win, scale);
+    pass2_rows<MODE>(a.s, a.k, e, H, r0, lane, L,
+                     min(kRowBlocks, (H - r0 + 31) >> 5), win, scale);
   }
 }
 
@@ -331,7 +342,7 @@ __device__ __forceinline__ RowTables warp_tables(char* base, int cap, int warp) 
 }
 
 template <int OP, int MODE, int ACC>
-__global__ void __launch_bounds__(kThreads, 2) k_tile(LaunchArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) k_tile(LaunchArgs a) {  // 2 CTAs x 16 warps per SM
   extern __shared__ __align__(16) char smem_raw[];
   const WorkItem it = a.items[blockIdx.x];
   int wx0, wy0, wx1, wy1;
@@ -357,17 +368,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_tile(LaunchArgs a) {
   __syncthreads();
   const SmemWin win{s_w, s_acc, wx0, wy0, WS};
   const int64_t end = it.begin + it.count;
-  // warps pull groups of 32 events from a shared counter until the item is done
+  // warps pull groups of kGrab events from a shared counter until the item is
+  // done (lanes < kGrab set the group's events up in parallel)
   for (;;) {
     int g = 0;
     if (lane == 0) g = atomicAdd(&s_next_group, 1);
     g = __shfl_sync(kFull, g, 0);
-    const int64_t base = it.begin + (int64_t)g * 32;
+    const int64_t base = it.begin + (int64_t)g * kGrab;
     if (base >= end) break;
     const int64_t ei = base + lane;
     EventF mine = {};
-    if (ei < end) event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], mine);
-    const int nh = (int)min((int64_t)32, end - base);
+    if (lane < kGrab && ei < end)
+      event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], mine);
+    const int nh = (int)min((int64_t)kGrab, end - base);
     for (int j = 0; j < nh; ++j) {
       const EventF e = shfl_event(mine, j);
       process_event<OP, MODE, ACC>(a, e, win, lane, base + j);

@@ -67,21 +67,25 @@ __device__ __forceinline__ EventRows event_rows(const ScannerF& s,
                                                 const EventF& e) {
   EventRows r;
   r.k4 = 4.0f * e.sec * e.sec * s.ipsdl;
-  r.inv2z = 0.5f / s.ipsz;
-  r.inv_pw = 1.0f / s.pw;
+  r.inv2z = s.inv2z;
+  r.inv_pw = s.inv_pw;
   r.x0 = (e.z - s.tl_z_half_w) * r.inv_pw;
   return r;
 }
 
-// Closed-form boundaries are trusted without an exact test when they lie at
-// least kEdgeMargin pixels from every pixel centre and the run is at least
-// kTrustWidth pixels wide.  There, the distance to the boundary changes q by
-// >= 2 C hw pw^2 kEdgeMargin >= 3e-3 (hw >= 2 px), while binary32 rounding
-// moves q by <= 9 (1+k)/(1-k) * 2^-21 ~ 1e-4 even for the most tilted
-// ellipses here (k = |B| / (2 sqrt(A C)) <= 0.93) and the closed form itself
-// is off by < 1e-3 px -- so the test's outcome is already decided.
-constexpr float kEdgeMargin = 0.02f;
-constexpr float kTrustWidth = 2.0f;
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Rows whose closed-form run is at least kWideRun pixels wide: the closed
+// form locates each end within ~1e-4 px (binary32 rounding of q is <= ~1e-4
+// even for the most tilted ellipses here, k = |B| / (2 sqrt(A C)) <= 0.93,
+// while q changes by >= 2 C hw pw^2 >= 0.03 per pixel), so each end is one of
+// two adjacent columns and two exact tests per end settle it -- no loop, no
+// divergence.  Narrower rows (the ellipse's tips) take the general search.
+constexpr float kWideRun = 1.0f;
 
 // Exact run of row iy within the box columns [tlx, brx): returns len, sets lo.
 __device__ __forceinline__ int row_run(const ScannerF& s, const EventF& e,
@@ -89,23 +93,22 @@ __device__ __forceinline__ int row_run(const ScannerF& s, const EventF& e,
                                        int& lo_out) {
   const int cmin = e.tlx, cmax = e.brx - 1;
   const float u = fmaf(-er.k4 * rs.dy, rs.dy, 9.0f);
-  const float hw = sqrtf(fmaxf(u, 0.0f) * er.inv2z) * er.inv_pw;
+  const float hw = sqrt_approx(fmaxf(u, 0.0f) * er.inv2z) * er.inv_pw;
   const float xv = fmaf(e.tan * rs.dy, er.inv_pw, er.x0);
   float xl = xv - hw, xh = xv + hw;
   int lo, hi;
-  if (hw >= kTrustWidth && fabsf(xl) < 1e7f && fabsf(xh) < 1e7f) {
-    const float cl = ceilf(xl), fh = floorf(xh);
-    const float dl = cl - xl, dh = xh - fh;  // in [0, 1]
-    lo = (int)cl;
-    hi = (int)fh;
-    const bool lo_ok = dl > kEdgeMargin && dl < 1.0f - kEdgeMargin;
-    const bool hi_ok = dh > kEdgeMargin && dh < 1.0f - kEdgeMargin;
-    if (lo_ok && hi_ok) {
-      lo = max(lo, cmin);
-      hi = min(hi, cmax);
-      lo_out = lo;
-      return hi >= lo ? hi - lo + 1 : 0;
-    }
+  if (hw >= kWideRun && fabsf(xv) < 1e7f) {
+    const int lc = (int)ceilf(xl), hc = (int)floorf(xh);
+    const bool a = in_ellipse(rs, e.C, col_dz(s, e, lc - 1));
+    const bool b = in_ellipse(rs, e.C, col_dz(s, e, lc));
+    const bool c = in_ellipse(rs, e.C, col_dz(s, e, hc));
+    const bool d = in_ellipse(rs, e.C, col_dz(s, e, hc + 1));
+    lo = a ? lc - 1 : (b ? lc : lc + 1);
+    hi = d ? hc + 1 : (c ? hc : hc - 1);
+    lo = max(lo, cmin);
+    hi = min(hi, cmax);
+    lo_out = lo;
+    return hi >= lo ? hi - lo + 1 : 0;
   }
   if (!(fabsf(xl) < 1e8f) || !(fabsf(xh) < 1e8f)) {
     lo = cmin;  // unusable closed form: scan the whole row
