@@ -148,7 +148,12 @@ Tiling choose_tiling(const strip_ctx* ctx, int max_w, int max_h) {
   t.row_cap = std::min(128, std::max(32, (max_h + 31) / 32 * 32));
   for (;;) {
     const int WX = std::min(n_z, TX + 2 * HX), WY = std::min(n_y, TY + 2 * HY);
-    const int WS = WX | 1;
+    // Row stride = 2 (mod 32): the 32 lanes of a warp walk runs on 32
+    // different rows, so a lane's bank is (row * WS + column) mod 32; of all
+    // residues, 2 (and 30) spread the middle-out-ranked rows of realistic
+    // ellipses over the banks best (fewest shared-memory wavefronts in a
+    // simulation over events of the 800 x 400 geometry).
+    const int WS = WX + ((2 - WX % 32) + 32) % 32;
     // groups of a block of row_cap rows whose runs fit a window row
     t.bit_words = (t.row_cap * ((WX + 2) / 3) + 31) / 32 + 1;
     const int bytes = tile_smem_bytes(WY, WS, t.row_cap, t.bit_words);
