@@ -180,6 +180,37 @@ int strip_debug_pixel_sets(strip_ctx* ctx, const float* z_u, const float* z_d,
                            const float* dl, int64_t n, int32_t* n_bb,
                            int32_t* n_in, uint64_t* digest);
 
+/* ---- allocation-free iteration ----------------------------------------- */
+
+/* Largest image (n_y * n_z pixels) strip_iterate_noalloc accepts. */
+#define STRIP_NOALLOC_MAX_PIXELS (1 << 20)
+
+/* One MLEM iteration that allocates no device memory, for callers that cannot
+ * call cudaMalloc: code inside a host framework that owns all device memory
+ * through its own pool under a fixed budget, and pipelines that must not hit
+ * cudaMalloc / cudaFree because they can synchronise the device.  No
+ * counterpart in the reference.
+ *
+ * Inputs and outputs are caller-owned DEVICE buffers on the current device:
+ * n events (z_u, z_d, dl), the image rho_in and the result rho_out
+ * (n_y * n_z floats each; rho_out may equal rho_in).  `mode` as
+ * strip_iterate; accumulation as STRIP_ACCUM_KAHAN.  The work is enqueued on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream) and the call
+ * returns without waiting for it.  Events are processed unbinned, one warp
+ * per event, straight from global memory.
+ *
+ * Scratch is a fixed file-scope device array (a binary64 accumulator and a
+ * binary32 sensitivity image of STRIP_NOALLOC_MAX_PIXELS entries each, 12 MiB
+ * held by every GPU that loads the library until exit).  The first call on a
+ * device looks up the scratch's device address, so make that first call
+ * before any stream capture.  All calls share the scratch: calls that overlap
+ * on the GPU race.  Images larger than STRIP_NOALLOC_MAX_PIXELS are rejected
+ * with STRIP_E_INVALID, as are invalid geometries and null pointers. */
+int strip_iterate_noalloc(const strip_geometry* geometry, const float* d_z_u,
+                          const float* d_z_d, const float* d_dl, int64_t n,
+                          const float* d_rho_in, float* d_rho_out, int mode,
+                          void* stream);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 
 /* Totals over the context's events of the bounding-box pixels tested and the

@@ -78,7 +78,11 @@ int fail(strip_ctx* c, int code, const char* fmt, ...) {
                   __FILE__, __LINE__);                                   \
   } while (0)
 
-int16_t narrow16(int32_t v) { return (int16_t)(uint16_t)(uint32_t)v; }
+}  // namespace
+
+namespace stripmlem {
+
+static int16_t narrow16(int32_t v) { return (int16_t)(uint16_t)(uint32_t)v; }
 
 // Scanner<float, short>(R, L, n_y, n_z, p_h, p_w, s_z, s_dl, c_y, c_z) and
 // GaussianKernel<float>(s_z, s_dl): scanner.h:50-67, gaussian_kernel.h:27-33.
@@ -124,6 +128,10 @@ KernelF make_kernel(double sigma_z, double sigma_dl, float pw) {
   k.lg2kc = (float)log2((double)k.kc);
   return k;
 }
+
+}  // namespace stripmlem
+
+namespace {
 
 template <class T>
 void dfree(T*& p) {

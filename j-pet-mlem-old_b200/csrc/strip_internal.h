@@ -77,6 +77,12 @@ struct LaunchArgs {
   int* status;           // device status word (0 = ok)
 };
 
+// ---- host helpers (strip_capi.cu) ------------------------------------------
+// Scanner<float, short> + GaussianKernel<float> constants of a geometry, and
+// the kernel constants of given model sigmas (pixel pitch pw).
+ScannerF make_scanner(const strip_geometry& g);
+KernelF make_kernel(double sigma_z, double sigma_dl, float pw);
+
 // ---- launchers (strip_kernels.cu) ----------------------------------------
 int tile_smem_bytes(int WYmax, int WS, int row_cap, int bit_words);
 int global_smem_bytes(int cap, int bit_words);
@@ -100,6 +106,10 @@ cudaError_t launch_global(int op, int mode, int accum, const LaunchArgs& a,
                           cudaStream_t st);
 cudaError_t launch_update(float* rho, double* acc, int64_t n_pix, double scale,
                           cudaStream_t st);
+// rho_out_j = rho_in_j * acc_j (acc is left as is)
+cudaError_t launch_update_out(const float* rho_in, float* rho_out,
+                              const double* acc, int64_t n_pix,
+                              cudaStream_t st);
 cudaError_t launch_sensitivity(const ScannerF& s, int five_point, float* out,
                                cudaStream_t st);
 cudaError_t launch_debug_sets(const ScannerF& s, const float* zu,

@@ -504,6 +504,13 @@ __global__ void k_bin_scatter(const int* keys, int64_t n, const float* zu,
   }
 }
 
+__global__ void k_update_out(const float* rho_in, float* rho_out,
+                             const double* acc, int64_t n) {
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (int64_t)gridDim.x * blockDim.x)
+    rho_out[j] = (float)((double)rho_in[j] * acc[j]);
+}
+
 __global__ void k_update(float* rho, double* acc, int64_t n, double scale) {
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
        j += (int64_t)gridDim.x * blockDim.x) {
@@ -748,6 +755,13 @@ cudaError_t launch_bin_scatter(const int* keys, int64_t n, const float* zu,
 cudaError_t launch_update(float* rho, double* acc, int64_t n_pix, double scale,
                           cudaStream_t st) {
   k_update<<<grid_for(n_pix), kThreads, 0, st>>>(rho, acc, n_pix, scale);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_update_out(const float* rho_in, float* rho_out,
+                              const double* acc, int64_t n_pix,
+                              cudaStream_t st) {
+  k_update_out<<<grid_for(n_pix), kThreads, 0, st>>>(rho_in, rho_out, acc, n_pix);
   return cudaGetLastError();
 }
 

@@ -120,6 +120,11 @@ SIGNATURES = {
         ctypes.c_int,
         [_ctx, _f, _f, _f, ctypes.c_int64, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_uint64)],
     ),
+    "strip_iterate_noalloc": (
+        ctypes.c_int,
+        [_P(Geometry), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p],
+    ),
     "strip_probe_fp32_peak": (ctypes.c_int, [ctypes.c_int, _d]),
     "strip_count_work": (
         ctypes.c_int,
