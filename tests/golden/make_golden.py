@@ -17,9 +17,13 @@ triples z_u z_d dl; images raw f32, n_y rows of n_z):
   metre.events.bin         2000 events in metres (the reference CLI defaults:
                            R 0.5, L 1, p 0.01, s_z 0.015, s_dl 0.06)
   metre.ref2.npz           reference image after 2 iterations (nocontract)
+  text.events.txt          1500 C1 events as text in mixed number formats
+  text.ref1.npz            reference image after 1 iteration of the text file
 """
 import os
+import subprocess
 import sys
+import tempfile
 
 import numpy as np
 
@@ -82,6 +86,29 @@ def main():
     orc.write_events_bin(os.path.join(HERE, "edge.events.bin"), ezu, ezd, edl)
     ei, _ = orc.run_ref(g, ezu, ezd, edl, 1, threads=1, nocontract=True)
     np.savez_compressed(os.path.join(HERE, "edge.ref1.npz"), nocontract=ei)
+
+    # text events: mixed number formats, '+' signs, exponents (the reference
+    # parser turns e>=2 into 10*0.1^(e-1)), and a last line without '\n'
+    tzu, tzd, tdl = sm.generate_events(sc, C1_PHANTOM, 1500, seed=12)
+    fmts = ["{:.6f}", "{:.3e}", "{:g}", "{:+.4f}", "{:.2E}", "{:.9f}"]
+    lines = []
+    for i in range(len(tzu)):
+        f = fmts[i % len(fmts)]
+        lines.append(" ".join(f.format(float(v)) for v in (tzu[i], tzd[i], tdl[i])))
+    lines[7] = "1.5e2 -2.0e1 3e-1"
+    lines[8] = "12 -7 0"
+    lines[9] = "+.5 -.25 10.125"
+    with open(os.path.join(HERE, "text.events.txt"), "w") as f:
+        f.write("\n".join(lines))  # no newline after the last line
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "r.bin")
+        exe = orc.REF_RECON_NOCONTRACT
+        subprocess.run([exe, os.path.join(HERE, "text.events.txt"), "-r", "200", "-l", "500",
+                        "-p", "2", "--n-y-pixels", "200", "--n-z-pixels", "250", "--s-z", "10",
+                        "--s-dl", "42", "-i", "1", "-I", "1", "-T", "1", "-o", out],
+                       check=True, capture_output=True)
+        ti = np.fromfile(os.path.join(td, "r_1.bin"), dtype="<f4").reshape(200, 250)
+    np.savez_compressed(os.path.join(HERE, "text.ref1.npz"), nocontract=ti)
 
     gm = orc.geometry(*METRE)
     scm = sm.Scanner(*METRE)
