@@ -45,9 +45,13 @@ PHANTOM = [
     (0, 0, 360, 175, 0, 0.2),
 ]
 SEED = 20260101
+# DRAM bytes (read + write) per event of one k_tile pass, from an ncu capture
+# of this workload's first 2e7 events (profiles/k_tile_strip_c2_2e7events.md:
+# 246.9 MB read + 7.9 MB written); the traffic grows with the event count.
+TILE_DRAM_BYTES_PER_EVENT = (246.890240e6 + 7.881472e6) / 2e7
 
 
-def workload_config(n_events, e2e_iters):
+def workload_config(n_events, e2e_iters, world=1):
     return {
         "workload": "strip MLEM, 800x400 image of 1 mm pixels, R=400 mm, L=800 mm, "
                     "sigma_z=5 mm, sigma_dl=25 mm, 10-ellipse Shepp-like phantom",
@@ -59,7 +63,10 @@ def workload_config(n_events, e2e_iters):
         "step": "one full-set MLEM iteration over all events",
         "e2e_step": f"set_events from pinned host + {e2e_iters} iterations + image D2H",
         "l2": "inputs (12 B/event, 2.4 GB) larger than the 126 MB L2; no flush",
-        "parallelism": "events sharded per rank, image replicated",
+        "parallelism": ("single GPU" if world == 1 else
+                        f"{world} ranks: events sharded per rank (each its own 2e8), "
+                        "image replicated, NCCL all-reduce of the binary64 "
+                        "backprojection every iteration"),
         "seed": SEED,
     }
 
@@ -68,6 +75,15 @@ def scanner():
     import stripmlem as sm
     return sm.Scanner(GEOM["radius"], GEOM["length"], GEOM["n_y"], GEOM["n_z"],
                       GEOM["p"], GEOM["p"], GEOM["s_z"], GEOM["s_dl"])
+
+
+def measured_peak(key):
+    """A peak of MEASURED_PEAKS.json (written per machine), or None."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)[key])
+    except Exception:
+        return None
 
 
 def host_cores():
@@ -184,7 +200,7 @@ def reference_arm(args, rank, world):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": n_sample / (value * 1e6) * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config(args.events, args.e2e_iters),
+        "config": workload_config(args.events, args.e2e_iters, world),
         "cpu_baseline": {"value": value, "unit": UNIT,
                          "cores": cores if kind == "reference" else 1,
                          "kind": kind, "sample": sample},
@@ -204,6 +220,41 @@ def pinned_empty(n):
     return t, t.numpy()
 
 
+def differentiable_throughput(rec, n, reps=2):
+    """Device time of the forward projection (strip_forward_device) and the
+    adjoint (strip_adjoint_device) over the resident events; returns ms of
+    each (mean over reps), at the geometry's sigmas."""
+    import torch
+    dev = rec.torch_device
+    n_pix = GEOM["n_y"] * GEOM["n_z"]
+    rho = torch.ones(n_pix, dtype=torch.float32, device=dev)
+    y = torch.empty(n, dtype=torch.float64, device=dev)
+    w = torch.empty(n, dtype=torch.float64, device=dev)
+    g = torch.empty(n_pix, dtype=torch.float64, device=dev)
+    sz, sdl = GEOM["s_z"], GEOM["s_dl"]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    tf = ta = 0.0
+    for r in range(reps + 1):
+        torch.cuda.synchronize()
+        ev[0].record()
+        rec._check(rec.lib.strip_forward_device(rec._ctx, rho.data_ptr(), sz, sdl, 0,
+                                                y.data_ptr()))
+        ev[1].record()
+        torch.reciprocal(y, out=w)
+        torch.cuda.synchronize()
+        ev[1].synchronize()
+        t_fwd = ev[0].elapsed_time(ev[1])
+        ev[0].record()
+        rec._check(rec.lib.strip_adjoint_device(rec._ctx, w.data_ptr(), sz, sdl, 0,
+                                                g.data_ptr()))
+        ev[2].record()
+        ev[2].synchronize()
+        if r > 0:  # the first pass is a warm-up
+            tf += t_fwd
+            ta += ev[0].elapsed_time(ev[2])
+    return tf / reps, ta / reps
+
+
 def ours(args, rank, world, local_rank):
     import torch
     import stripmlem as sm
@@ -212,7 +263,9 @@ def ours(args, rank, world, local_rank):
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
     torch.cuda.set_device(local_rank)
     sc = scanner()
     n = args.events
@@ -235,7 +288,6 @@ def ours(args, rank, world, local_rank):
     rec = sm.Reconstruction(sc, device=local_rank, mode=sm.MODE_CPU,
                             accumulation=sm.ACCUM_KAHAN)
     rec.set_events(zu, zd, dl)
-    st = rec.stats()
     work_bb, work_in, nonempty = [ctypes.c_int64() for _ in range(3)]
     rec._check(rec.lib.strip_count_work(rec._ctx, ctypes.byref(work_bb),
                                         ctypes.byref(work_in), ctypes.byref(nonempty)))
@@ -244,19 +296,41 @@ def ours(args, rank, world, local_rank):
     peak = ctypes.c_double()
     rec._check(rec.lib.strip_probe_fp32_peak(local_rank, ctypes.byref(peak)))
 
-    # warm-up, then K timed iterations in one call (device time on the
-    # library's stream, CUDA events on both sides, synchronised)
-    rec(None, args.warmup)
+    # N = 1: strip_iterate runs the K iterations in one call.  N > 1: each
+    # iteration is strip_accumulate on the rank's events, an NCCL all-reduce
+    # of the binary64 accumulator, and strip_update on every rank.
+    shd = None
+    if world > 1:
+        from stripmlem.distributed import ShardedReconstruction
+        shd = ShardedReconstruction(rec, exchange="device")
+
+    def iterate(k):
+        if shd is None:
+            rec(None, k)
+        else:
+            shd(k)
+
+    iterate(args.warmup)
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local_rank) as clk:
-        rec(None, args.steps)
+        t0.record()
+        iterate(args.steps)
+        t1.record()
         torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
     st = rec.stats()
-    t_ms = st["last_iterate_ms"]
-    tile_ms = st["last_tile_ms"]
-    launches = st["kernel_launches"]
+    if shd is None:
+        t_ms = st["last_iterate_ms"]   # library stream, CUDA events
+        tile_ms = st["last_tile_ms"]
+        launches = st["kernel_launches"]
+    else:
+        t_ms = t0.elapsed_time(t1)
+        tile_ms = None
+        launches = None
     if dist is not None:
         tt = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -264,26 +338,55 @@ def ours(args, rank, world, local_rank):
     value = world * n * args.steps / (t_ms / 1e3) / 1e6
     clocks = clk.summary()
 
+    # the tile kernel's own time: from the multi-rank run when N = 1, else
+    # from one more local pass of the same events
+    if tile_ms is None:
+        rec(None, 1)
+        st1 = rec.stats()
+        tile_ms = st1["last_tile_ms"] * args.steps
+        launches = st1["kernel_launches"] * args.steps  # tile (+ global) + update
+
     # end to end through the public API with host buffers
     e2e = None
     if args.e2e_steps > 0:
         img = np.empty((GEOM["n_y"], GEOM["n_z"]), np.float32)
         times = []
         for s in range(args.e2e_steps + 1):
+            if dist is not None:
+                dist.barrier()
             torch.cuda.synchronize()
-            t0 = time.perf_counter()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
             rec.set_events(zu, zd, dl)
             rec.rho = np.ones_like(img)
-            rec(None, args.e2e_iters)
+            iterate(args.e2e_iters)
             img[...] = rec.rho
+            b.record()
             torch.cuda.synchronize()
             if s > 0:
-                times.append(time.perf_counter() - t0)
-        e2e_t = max(times) if dist is None else max(times)
-        e2e = {"value": world * n * args.e2e_iters / (sum(times) / len(times)) / 1e6,
+                times.append(a.elapsed_time(b) / 1e3)
+        e2e_t = sum(times) / len(times)
+        if dist is not None:
+            tt = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_t = float(tt.item())
+        e2e = {"value": world * n * args.e2e_iters / e2e_t / 1e6,
                "unit": UNIT, "h2d_bytes_per_step": int(3 * 4 * n),
                "d2h_bytes_per_step": int(img.nbytes), "steps": len(times),
-               "iterations_per_step": args.e2e_iters}
+               "iterations_per_step": args.e2e_iters,
+               "timed": "set_events (pinned host -> HBM, binning) + iterations + image D2H, "
+                        "CUDA events, max over ranks"}
+
+    diff = None
+    if world == 1 and not args.no_differentiable:
+        tf, ta = differentiable_throughput(rec, n)
+        mlem_ms = t_ms / args.steps
+        diff = {"forward_ms": tf, "adjoint_ms": ta,
+                "forward_plus_adjoint_Mevent_per_s": n / ((tf + ta) / 1e3) / 1e6,
+                "mlem_Mevent_per_s": n / (mlem_ms / 1e3) / 1e6,
+                "ratio_vs_mlem": mlem_ms / (tf + ta),
+                "what": "strip_forward_device then strip_adjoint_device over the same "
+                        "events (y_e = sum_j K_ej rho_j, g_j = sum_e K_ej / y_e)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -294,16 +397,23 @@ def ours(args, rank, world, local_rank):
                "kind": kind, "sample": sample}
 
     achieved = flops_per_iter / (tile_ms / args.steps / 1e3) / 1e12
+    hbm_peak = measured_peak("hbm_gbs")
+    hbm_achieved = (12 * n) / (tile_ms / args.steps / 1e3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": workload_config(n, args.e2e_iters),
+        "config": workload_config(n, args.e2e_iters, world),
         "roofline": {
             "bound": "fp32", "achieved": achieved, "peak": peak.value,
             "unit": "TFLOP/s", "frac": achieved / peak.value if peak.value else None,
-            "traffic": None,
+            "traffic": TILE_DRAM_BYTES_PER_EVENT * n,
+            "traffic_unit": "bytes per launch (ncu capture at 2e7 events, scaled)",
+            "algorithmic_bytes": 12 * n + 4 * GEOM["n_y"] * GEOM["n_z"],
+            "hbm": {"achieved_gbs": hbm_achieved, "peak_gbs": hbm_peak,
+                    "frac": hbm_achieved / hbm_peak if hbm_peak else None,
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
             "kernel": "k_tile (tile-window MLEM kernel)",
             "work_model": "10 flops per bbox pixel + 18 per in-ellipse pixel",
             "bbox_pixels_per_iter": work_bb.value, "ellipse_pixels_per_iter": work_in.value,
@@ -320,8 +430,12 @@ def ours(args, rank, world, local_rank):
         line["e2e"] = e2e
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if diff is not None:
+        line["differentiable"] = diff
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if shd is not None:
+        shd.close()
     rec.close()
     if dist is not None:
         dist.destroy_process_group()
@@ -339,6 +453,7 @@ def main():
     ap.add_argument("--e2e-iters", type=int, default=20)
     ap.add_argument("--ref-events", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-differentiable", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", 0))

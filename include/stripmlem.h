@@ -155,6 +155,29 @@ int strip_get_sensitivity(strip_ctx* ctx, int five_point, float* out);
 int strip_iterate(strip_ctx* ctx, int n_iter, int mode, int n_subsets,
                   int first, strip_progress_cb progress, void* user);
 
+/* ---- split iteration: one MLEM/OSEM step as backprojection + update ----
+ * For event sets sharded over several processes or GPUs, each holding the
+ * same image: every shard runs strip_accumulate for the subset, the shards
+ * sum their accumulators (an all-reduce of n_y * n_z binary64 values, e.g.
+ * ncclAllReduce on the buffer given to strip_set_accumulator), and every
+ * shard applies strip_update.  One strip_iterate step of n_subsets == 1 is
+ * strip_accumulate(ctx, mode, 1, 0) followed by strip_update(ctx, 1.0); an
+ * OSEM step visits s = 0 .. n_subsets - 1, each followed by an update with
+ * scale n_subsets.  The reference's loop is single-process
+ * (reconstruction.h:109-154); its per-thread images summed before the update
+ * (reconstruction.h:137-148) are the single-node form of this exchange. */
+
+/* Makes the caller's DEVICE buffer of n_y * n_z binary64 values (on the
+ * context's device) the backprojection accumulator of every later call, and
+ * zero-fills it; NULL returns to the context's own buffer.  The caller keeps
+ * the buffer alive while it is in use. */
+int strip_set_accumulator(strip_ctx* ctx, double* d_acc);
+/* acc_j += sum_{e in subset} P_ej / D_e over the context's events of subset
+ * `subset` (event e belongs to subset e % n_subsets); rho is not changed. */
+int strip_accumulate(strip_ctx* ctx, int mode, int n_subsets, int subset);
+/* rho_j <- rho_j * acc_j * scale, then acc_j <- 0. */
+int strip_update(strip_ctx* ctx, double scale);
+
 /* ---- differentiable projections (pixel sets fixed by the geometry's sigmas) */
 
 /* y_e = sum_j P_ej rho_j for every event, in the caller's event order, with
@@ -168,6 +191,18 @@ int strip_adjoint(strip_ctx* ctx, const double* w, double sigma_z,
 int strip_grad_sigma(strip_ctx* ctx, const float* rho, const double* w,
                      double sigma_z, double sigma_dl, double* d_sigma_z,
                      double* d_sigma_dl);
+/* The same three with DEVICE buffers on the context's device (rho: n_y * n_z
+ * floats, y and w: one double per event of set_events, g: n_y * n_z doubles,
+ * grad: 2 doubles {d/dsigma_z, d/dsigma_dl}); no host copies.  The reference
+ * has no projection operators; these serve a differentiable model whose
+ * tensors live on the GPU. */
+int strip_forward_device(strip_ctx* ctx, const float* d_rho, double sigma_z,
+                         double sigma_dl, int mode, double* d_y);
+int strip_adjoint_device(strip_ctx* ctx, const double* d_w, double sigma_z,
+                         double sigma_dl, int mode, double* d_g);
+int strip_grad_sigma_device(strip_ctx* ctx, const float* d_rho,
+                            const double* d_w, double sigma_z,
+                            double sigma_dl, double* d_grad);
 
 /* ---- parity ----------------------------------------------------------- */
 
@@ -247,6 +282,19 @@ typedef struct strip_ellipse {
 int strip_generate_events(const strip_geometry* g, const strip_ellipse* ellipses,
                           int n_ellipses, uint64_t seed, int64_t n,
                           float* z_u, float* z_d, float* dl);
+
+/* Same detection and smearing with emission points drawn from an activity
+ * image rho (n_y * n_z, the image layout above, non-negative): pixel with
+ * probability rho_j / sum rho, point uniform in the pixel.  uniform_angle = 0
+ * draws tan(theta) uniformly over the acceptance as above; 1 draws the angle
+ * uniformly in (-pi/2, pi/2) as the reference's phantom tool does
+ * (phantom.h:213), the emission model the strip kernel assumes.  The
+ * reference generates only from phantom shapes (phantom.h:120-215); an image
+ * source is what a list-mode model fit needs, where rho is the truth the
+ * forward projection is evaluated on. */
+int strip_generate_events_image(const strip_geometry* g, const float* rho,
+                                uint64_t seed, int64_t n, int uniform_angle,
+                                float* z_u, float* z_d, float* dl);
 
 #ifdef __cplusplus
 }

@@ -32,7 +32,8 @@ struct strip_ctx {
   int accum = STRIP_ACCUM_KAHAN;
   int64_t n_pix = 0;
   float* d_rho = nullptr;
-  double* d_acc = nullptr;
+  double* d_acc = nullptr;      // accumulator in use (own or the caller's)
+  double* d_acc_own = nullptr;  // the context's own accumulator
   float* d_sens5 = nullptr;
   // binned events
   int64_t n_events = 0;   // as given by the caller
@@ -392,6 +393,32 @@ LaunchArgs base_args(strip_ctx* ctx) {
   return a;
 }
 
+// Re-bins the resident events for n_subsets OSEM subsets when the current
+// binning differs: the binned arrays become the input, perm keeps the
+// caller's indices.
+int ensure_binning(strip_ctx* ctx, int n_subsets) {
+  if (n_subsets == ctx->n_subsets) return STRIP_OK;
+  float* zu = ctx->d_zu;
+  float* zd = ctx->d_zd;
+  float* dl = ctx->d_dl;
+  int64_t* pm = ctx->d_perm;
+  ctx->d_zu = ctx->d_zd = ctx->d_dl = nullptr;
+  ctx->d_perm = nullptr;
+  const int rc = bin_events(ctx, zu, zd, dl, pm, ctx->n_binned, n_subsets);
+  if (rc != STRIP_OK) {
+    ctx->d_zu = zu;
+    ctx->d_zd = zd;
+    ctx->d_dl = dl;
+    ctx->d_perm = pm;
+    return rc;
+  }
+  cudaFree(zu);
+  cudaFree(zd);
+  cudaFree(dl);
+  cudaFree(pm);
+  return STRIP_OK;
+}
+
 // Runs op over every subset's work items and global-path events.
 int run_all(strip_ctx* ctx, int op, int mode, LaunchArgs a) {
   for (int sb = 0; sb < ctx->n_subsets; ++sb) {
@@ -440,8 +467,9 @@ int strip_ctx_create(const strip_geometry* g, int device, strip_ctx** out) {
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
     if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
     if (cudaMalloc(&ctx->d_rho, ctx->n_pix * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&ctx->d_acc, ctx->n_pix * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_acc_own, ctx->n_pix * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&ctx->d_status, sizeof(int)) != cudaSuccess) { rc = STRIP_E_NOMEM; break; }
+    ctx->d_acc = ctx->d_acc_own;
     std::vector<float> ones((size_t)ctx->n_pix, 1.0f);  // reconstruction.h:59
     if (cudaMemcpy(ctx->d_rho, ones.data(), ctx->n_pix * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(ctx->d_acc, 0, ctx->n_pix * sizeof(double)) != cudaSuccess ||
@@ -461,7 +489,7 @@ int strip_ctx_destroy(strip_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   dfree(ctx->d_rho);
-  dfree(ctx->d_acc);
+  dfree(ctx->d_acc_own);
   dfree(ctx->d_sens5);
   dfree(ctx->d_zu);
   dfree(ctx->d_zd);
@@ -599,27 +627,7 @@ int strip_iterate(strip_ctx* ctx, int n_iter, int mode, int n_subsets,
       n_subsets < 1 || n_subsets > 4096)
     return fail(ctx, STRIP_E_INVALID, "invalid iterate arguments");
   if (int rc = set_device(ctx)) return rc;
-  if (n_subsets != ctx->n_subsets) {
-    // re-bin: the binned arrays become the input, perm keeps caller indices
-    float* zu = ctx->d_zu;
-    float* zd = ctx->d_zd;
-    float* dl = ctx->d_dl;
-    int64_t* pm = ctx->d_perm;
-    ctx->d_zu = ctx->d_zd = ctx->d_dl = nullptr;
-    ctx->d_perm = nullptr;
-    int rc = bin_events(ctx, zu, zd, dl, pm, ctx->n_binned, n_subsets);
-    if (rc != STRIP_OK) {
-      ctx->d_zu = zu;
-      ctx->d_zd = zd;
-      ctx->d_dl = dl;
-      ctx->d_perm = pm;
-      return rc;
-    }
-    cudaFree(zu);
-    cudaFree(zd);
-    cudaFree(dl);
-    cudaFree(pm);
-  }
+  if (int rc = ensure_binning(ctx, n_subsets)) return rc;
   if (mode == STRIP_MODE_GPU)
     if (int rc = ensure_sens5(ctx)) return rc;
   LaunchArgs a = base_args(ctx);
@@ -678,90 +686,231 @@ int strip_iterate(strip_ctx* ctx, int n_iter, int mode, int n_subsets,
   return STRIP_OK;
 }
 
-int strip_forward(strip_ctx* ctx, const float* rho, double sigma_z,
-                  double sigma_dl, int mode, double* y) {
+int strip_set_accumulator(strip_ctx* ctx, double* d_acc) {
+  if (!ctx) return STRIP_E_INVALID;
+  if (int rc = set_device(ctx)) return rc;
+  if (d_acc) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, d_acc) != cudaSuccess ||
+        at.type != cudaMemoryTypeDevice || at.device != ctx->device) {
+      cudaGetLastError();
+      return fail(ctx, STRIP_E_INVALID,
+                  "strip_set_accumulator: not device memory of this context's device");
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->d_acc = d_acc ? d_acc : ctx->d_acc_own;
+  CK(cudaMemsetAsync(ctx->d_acc, 0, ctx->n_pix * sizeof(double), ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return STRIP_OK;
+}
+
+int strip_accumulate(strip_ctx* ctx, int mode, int n_subsets, int subset) {
   if (int rc = check_ready(ctx)) return rc;
-  if (!rho || !y || !(sigma_z > 0) || !(sigma_dl > 0) ||
+  if ((mode != STRIP_MODE_CPU && mode != STRIP_MODE_GPU) || n_subsets < 1 ||
+      n_subsets > 4096 || subset < 0 || subset >= n_subsets)
+    return fail(ctx, STRIP_E_INVALID, "invalid accumulate arguments");
+  if (int rc = set_device(ctx)) return rc;
+  if (int rc = ensure_binning(ctx, n_subsets)) return rc;
+  if (mode == STRIP_MODE_GPU)
+    if (int rc = ensure_sens5(ctx)) return rc;
+  LaunchArgs a = base_args(ctx);
+  a.sens = (mode == STRIP_MODE_GPU) ? ctx->d_sens5 : nullptr;
+  a.items = ctx->d_items + ctx->sub_item_begin[subset];
+  a.n_items = ctx->sub_item_count[subset];
+  a.g_begin = ctx->sub_g_begin[subset];
+  a.g_count = ctx->sub_g_count[subset];
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  CK(launch_tile(OP_MLEM, mode, ctx->accum, a, ctx->stream));
+  CK(launch_global(OP_MLEM, mode, ctx->accum, a, ctx->stream));
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  ctx->stats.last_iterate_ms = ms;
+  ctx->stats.last_tile_ms = ms;
+  ctx->stats.kernel_launches = (a.n_items > 0) + (a.g_count > 0);
+  return STRIP_OK;
+}
+
+int strip_update(strip_ctx* ctx, double scale) {
+  if (!ctx) return STRIP_E_INVALID;
+  if (!(scale > 0) || !std::isfinite(scale))
+    return fail(ctx, STRIP_E_INVALID, "invalid update scale");
+  if (int rc = set_device(ctx)) return rc;
+  CK(launch_update(ctx->d_rho, ctx->d_acc, ctx->n_pix, scale, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return STRIP_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+bool valid_sigmas(double sz, double sdl) {
+  return sz > 0 && sdl > 0 && std::isfinite(sz) && std::isfinite(sdl);
+}
+
+// The device-buffer cores of the projections: enqueue on the context stream,
+// no synchronisation.
+int forward_dev(strip_ctx* ctx, const float* d_rho, double sz, double sdl,
+                int mode, double* d_y) {
+  if (mode == STRIP_MODE_GPU)
+    if (int rc = ensure_sens5(ctx)) return rc;
+  CK(cudaMemsetAsync(d_y, 0, ctx->n_events * sizeof(double), ctx->stream));
+  LaunchArgs a = base_args(ctx);
+  a.k = make_kernel(sz, sdl, ctx->s.pw);
+  a.rho = d_rho;
+  a.sens = (mode == STRIP_MODE_GPU) ? ctx->d_sens5 : nullptr;
+  a.y_out = d_y;
+  return run_all(ctx, OP_FORWARD, mode, a);
+}
+
+int adjoint_dev(strip_ctx* ctx, const double* d_w, double sz, double sdl,
+                int mode, double* d_g) {
+  if (mode == STRIP_MODE_GPU)
+    if (int rc = ensure_sens5(ctx)) return rc;
+  CK(cudaMemsetAsync(d_g, 0, ctx->n_pix * sizeof(double), ctx->stream));
+  LaunchArgs a = base_args(ctx);
+  a.k = make_kernel(sz, sdl, ctx->s.pw);
+  a.acc = d_g;
+  a.w_in = d_w;
+  if (int rc = run_all(ctx, OP_ADJOINT, mode, a)) return rc;
+  if (mode == STRIP_MODE_GPU)
+    CK(launch_scale_copy(d_g, ctx->d_sens5, d_g, ctx->n_pix, ctx->stream));
+  return STRIP_OK;
+}
+
+int grad_dev(strip_ctx* ctx, const float* d_rho, const double* d_w, double sz,
+             double sdl, double* d_out2) {
+  CK(cudaMemsetAsync(d_out2, 0, 2 * sizeof(double), ctx->stream));
+  LaunchArgs a = base_args(ctx);
+  a.k = make_kernel(sz, sdl, ctx->s.pw);
+  a.rho = d_rho;
+  a.w_in = d_w;
+  a.grad_out = d_out2;
+  a.sz = sz;
+  a.sdl = sdl;
+  return run_all(ctx, OP_GRAD, STRIP_MODE_CPU, a);
+}
+
+// Device scratch of a host-buffer call, freed on every path.
+struct Scratch {
+  std::vector<void*> p;
+  ~Scratch() {
+    for (void* q : p) cudaFree(q);
+  }
+  template <class T>
+  cudaError_t get(T** out, int64_t count) {
+    void* q = nullptr;
+    const cudaError_t e = cudaMalloc(&q, std::max<int64_t>(count, 1) * sizeof(T));
+    if (e == cudaSuccess) p.push_back(q);
+    *out = static_cast<T*>(q);
+    return e;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int strip_forward_device(strip_ctx* ctx, const float* d_rho, double sigma_z,
+                         double sigma_dl, int mode, double* d_y) {
+  if (int rc = check_ready(ctx)) return rc;
+  if (!d_rho || !d_y || !valid_sigmas(sigma_z, sigma_dl) ||
       (mode != STRIP_MODE_CPU && mode != STRIP_MODE_GPU))
     return fail(ctx, STRIP_E_INVALID, "invalid forward arguments");
   if (int rc = set_device(ctx)) return rc;
-  if (mode == STRIP_MODE_GPU)
-    if (int rc = ensure_sens5(ctx)) return rc;
-  float* d_img = nullptr;
-  double* d_y = nullptr;
-  CK(cudaMalloc(&d_img, ctx->n_pix * sizeof(float)));
-  cudaError_t e = cudaMalloc(&d_y, std::max<int64_t>(ctx->n_events, 1) * sizeof(double));
-  if (e == cudaSuccess) e = cudaMemcpyAsync(d_img, rho, ctx->n_pix * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(d_y, 0, std::max<int64_t>(ctx->n_events, 1) * sizeof(double), ctx->stream);
-  int rc = STRIP_OK;
-  if (e == cudaSuccess) {
-    LaunchArgs a = base_args(ctx);
-    a.k = make_kernel(sigma_z, sigma_dl, ctx->s.pw);
-    a.rho = d_img;
-    a.sens = (mode == STRIP_MODE_GPU) ? ctx->d_sens5 : nullptr;
-    a.y_out = d_y;
-    rc = run_all(ctx, OP_FORWARD, mode, a);
-    if (rc == STRIP_OK && ctx->n_events > 0)
-      e = cudaMemcpyAsync(y, d_y, ctx->n_events * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  }
-  cudaFree(d_img);
-  cudaFree(d_y);
-  if (rc != STRIP_OK) return rc;
-  CK(e);
+  if (int rc = forward_dev(ctx, d_rho, sigma_z, sigma_dl, mode, d_y)) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return STRIP_OK;
+}
+
+int strip_adjoint_device(strip_ctx* ctx, const double* d_w, double sigma_z,
+                         double sigma_dl, int mode, double* d_g) {
+  if (int rc = check_ready(ctx)) return rc;
+  if (!d_w || !d_g || !valid_sigmas(sigma_z, sigma_dl) ||
+      (mode != STRIP_MODE_CPU && mode != STRIP_MODE_GPU))
+    return fail(ctx, STRIP_E_INVALID, "invalid adjoint arguments");
+  if (int rc = set_device(ctx)) return rc;
+  if (int rc = adjoint_dev(ctx, d_w, sigma_z, sigma_dl, mode, d_g)) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return STRIP_OK;
+}
+
+int strip_grad_sigma_device(strip_ctx* ctx, const float* d_rho,
+                            const double* d_w, double sigma_z,
+                            double sigma_dl, double* d_grad) {
+  if (int rc = check_ready(ctx)) return rc;
+  if (!d_rho || !d_w || !d_grad || !valid_sigmas(sigma_z, sigma_dl))
+    return fail(ctx, STRIP_E_INVALID, "invalid grad_sigma arguments");
+  if (int rc = set_device(ctx)) return rc;
+  if (int rc = grad_dev(ctx, d_rho, d_w, sigma_z, sigma_dl, d_grad)) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return STRIP_OK;
+}
+
+int strip_forward(strip_ctx* ctx, const float* rho, double sigma_z,
+                  double sigma_dl, int mode, double* y) {
+  if (int rc = check_ready(ctx)) return rc;
+  if (!rho || !y || !valid_sigmas(sigma_z, sigma_dl) ||
+      (mode != STRIP_MODE_CPU && mode != STRIP_MODE_GPU))
+    return fail(ctx, STRIP_E_INVALID, "invalid forward arguments");
+  if (int rc = set_device(ctx)) return rc;
+  Scratch sc;
+  float* d_img;
+  double* d_y;
+  CK(sc.get(&d_img, ctx->n_pix));
+  CK(sc.get(&d_y, ctx->n_events));
+  CK(cudaMemcpyAsync(d_img, rho, ctx->n_pix * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  if (int rc = forward_dev(ctx, d_img, sigma_z, sigma_dl, mode, d_y)) return rc;
+  CK(cudaMemcpyAsync(y, d_y, ctx->n_events * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   return STRIP_OK;
 }
 
 int strip_adjoint(strip_ctx* ctx, const double* w, double sigma_z,
                   double sigma_dl, int mode, double* g) {
   if (int rc = check_ready(ctx)) return rc;
-  if (!w || !g || !(sigma_z > 0) || !(sigma_dl > 0) ||
+  if (!w || !g || !valid_sigmas(sigma_z, sigma_dl) ||
       (mode != STRIP_MODE_CPU && mode != STRIP_MODE_GPU))
     return fail(ctx, STRIP_E_INVALID, "invalid adjoint arguments");
   if (int rc = set_device(ctx)) return rc;
-  if (mode == STRIP_MODE_GPU)
-    if (int rc = ensure_sens5(ctx)) return rc;
-  double* d_w = nullptr;
-  double* d_acc = nullptr;
-  double* d_out = nullptr;
-  const int64_t ne = std::max<int64_t>(ctx->n_events, 1);
-  cudaError_t e = cudaMalloc(&d_w, ne * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&d_acc, ctx->n_pix * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&d_out, ctx->n_pix * sizeof(double));
-  if (e == cudaSuccess && ctx->n_events > 0)
-    e = cudaMemcpyAsync(d_w, w, ctx->n_events * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(d_acc, 0, ctx->n_pix * sizeof(double), ctx->stream);
-  int rc = STRIP_OK;
-  if (e == cudaSuccess) {
-    LaunchArgs a = base_args(ctx);
-    a.k = make_kernel(sigma_z, sigma_dl, ctx->s.pw);
-    a.acc = d_acc;
-    a.w_in = d_w;
-    rc = run_all(ctx, OP_ADJOINT, mode, a);
-    if (rc == STRIP_OK)
-      e = launch_scale_copy(d_acc, mode == STRIP_MODE_GPU ? ctx->d_sens5 : nullptr, d_out, ctx->n_pix, ctx->stream);
-    if (rc == STRIP_OK && e == cudaSuccess)
-      e = cudaMemcpyAsync(g, d_out, ctx->n_pix * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  }
-  cudaFree(d_w);
-  cudaFree(d_acc);
-  cudaFree(d_out);
-  if (rc != STRIP_OK) return rc;
-  CK(e);
+  Scratch sc;
+  double* d_w;
+  double* d_g;
+  CK(sc.get(&d_w, ctx->n_events));
+  CK(sc.get(&d_g, ctx->n_pix));
+  CK(cudaMemcpyAsync(d_w, w, ctx->n_events * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  if (int rc = adjoint_dev(ctx, d_w, sigma_z, sigma_dl, mode, d_g)) return rc;
+  CK(cudaMemcpyAsync(g, d_g, ctx->n_pix * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   return STRIP_OK;
 }
 
 int strip_grad_sigma(strip_ctx* ctx, const float* rho, const double* w,
                      double sigma_z, double sigma_dl, double* d_sigma_z,
                      double* d_sigma_dl) {
-  (void)rho;
-  (void)w;
-  (void)sigma_z;
-  (void)sigma_dl;
-  (void)d_sigma_z;
-  (void)d_sigma_dl;
-  return fail(ctx, STRIP_E_STATE, "strip_grad_sigma: not available yet");
+  if (int rc = check_ready(ctx)) return rc;
+  if (!rho || !w || !d_sigma_z || !d_sigma_dl || !valid_sigmas(sigma_z, sigma_dl))
+    return fail(ctx, STRIP_E_INVALID, "invalid grad_sigma arguments");
+  if (int rc = set_device(ctx)) return rc;
+  Scratch sc;
+  float* d_img;
+  double* d_w;
+  double* d_g;
+  CK(sc.get(&d_img, ctx->n_pix));
+  CK(sc.get(&d_w, ctx->n_events));
+  CK(sc.get(&d_g, 2));
+  CK(cudaMemcpyAsync(d_img, rho, ctx->n_pix * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(d_w, w, ctx->n_events * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  if (int rc = grad_dev(ctx, d_img, d_w, sigma_z, sigma_dl, d_g)) return rc;
+  double g[2];
+  CK(cudaMemcpyAsync(g, d_g, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *d_sigma_z = g[0];
+  *d_sigma_dl = g[1];
+  return STRIP_OK;
 }
 
 int strip_count_work(strip_ctx* ctx, int64_t* n_bb, int64_t* n_in,

@@ -72,7 +72,7 @@ struct LaunchArgs {
   double* y_out;         // OP_FORWARD: per event (caller order)
   const double* w_in;    // OP_ADJOINT / OP_GRAD: per event weights (caller order)
   double* grad_out;      // OP_GRAD: 2 doubles (atomic)
-  float sz, sdl;         // OP_GRAD: model sigmas
+  double sz, sdl;        // OP_GRAD: model sigmas
   int gcap, gbit_words;  // event tables of the global path
   int* status;           // device status word (0 = ok)
 };

@@ -72,6 +72,32 @@ struct GaussRow {
   }
 };
 
+// GaussianKernel row with the sigma derivatives of log K.  With
+// N = a'Sa = ipsz a_pq + ipsdl a_r^2 (a_pq = ap^2 + aq^2) and kc ~ 1/(sz^2 sdl):
+//   sz  * dlogK/dsz  = -2 + ipsz a_pq / N + 2 ipsz t^2   = fz  + 2 ipsz t^2
+//   sdl * dlogK/dsdl = -1 + ipsdl a_r^2 / N + ipsdl b_r^2 = fdl
+struct GaussGradRow {
+  float pref, c0, dytan, fz, fdl;
+  __device__ __forceinline__ void init(const KernelF& k, float R, float y,
+                                       float tan, float sec, float dy) {
+    const float sec_sq = sec * sec;
+    const float yp = dy + y;
+    const float ap = -(yp - R) * sec_sq;
+    const float aq = -(yp + R) * sec_sq;
+    const float ar = -2.0f * yp * sec * tan;
+    const float apq = k.ipsz * (ap * ap + aq * aq);
+    const float arr = k.ipsdl * (ar * ar);
+    const float norm = apq + arr;
+    const float br = -2.0f * dy * sec;
+    const float brr = k.ipsdl * (br * br);
+    pref = k.kc * rsqrt_approx(norm);
+    c0 = -0.5f * kLog2e * brr;
+    dytan = dy * tan;
+    fz = apq / norm - 2.0f;
+    fdl = arr / norm + brr - 1.0f;
+  }
+};
+
 // AnalyticKernel, one row:  with t = dz - dy tan
 //   norm  = a'Sa + 2 o'Sb = n0 + n1 t
 //   b'Sa  = u1 t + u0

@@ -297,6 +297,52 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
   }
 }
 
+// OP_GRAD, GaussianKernel: adds w_e * d/d(sz, sdl) sum_j K_j w_j to
+// grad_out[0..1].  Lane per row (plain order); per row the run is walked with
+// the same recurrence as pass 1 while s0 = sum E w and s2 = sum E w t^2 are
+// gathered, so the row's share is pref * (fz s0 + 2 ipsz s2) / sz and
+// pref * fdl * s0 / sdl.
+template <class Win>
+__device__ __forceinline__ void grad_event(const LaunchArgs& a,
+                                           const EventF& e,
+                                           const EventRows& er, int H,
+                                           const Win& win, int lane,
+                                           int64_t pos) {
+  const double w = a.w_in[a.perm[pos]];
+  if (w == 0.0) return;
+  double gz = 0.0, gdl = 0.0;
+  for (int i = lane; i < H; i += 32) {
+    const int iy = e.tly + i;
+    const RowSet rs = row_set(a.s, e, iy);
+    int lo;
+    const int len = row_run(a.s, e, er, rs, lo);
+    if (len <= 0) continue;
+    GaussGradRow g;
+    g.init(a.k, a.s.R, e.y, e.tan, e.sec, rs.dy);
+    const float t0 = fmaf((float)lo, a.s.pw, a.s.tl_z_half_w) - e.z - g.dytan;
+    float E = ex2_approx(fmaf(a.k.c1 * t0, t0, g.c0));
+    float R = ex2_approx(fmaf(a.k.r1, t0, a.k.r0));
+    const auto p = win.ptr(iy, lo);
+    float s0 = 0.0f, s2 = 0.0f;
+    for (int j = 0; j < len; ++j) {
+      const float ew = E * win.read(p, j);
+      const float t = fmaf((float)j, a.s.pw, t0);
+      s0 += ew;
+      s2 = fmaf(ew * t, t, s2);
+      E *= R;
+      R *= a.k.q;
+    }
+    gz += (double)(g.pref * fmaf(g.fz, s0, 2.0f * a.k.ipsz * s2));
+    gdl += (double)(g.pref * g.fdl * s0);
+  }
+  gz = warp_sum(gz);
+  gdl = warp_sum(gdl);
+  if (lane == 0) {
+    atomicAdd(a.grad_out, w * gz / a.sz);
+    atomicAdd(a.grad_out + 1, w * gdl / a.sdl);
+  }
+}
+
 template <int OP, int MODE, int ACC, class Win>
 __device__ __forceinline__ void process_event(const LaunchArgs& a,
                                               const EventF& e, const Win& win,
@@ -304,6 +350,10 @@ __device__ __forceinline__ void process_event(const LaunchArgs& a,
   const int H = e.bry - e.tly;
   if (H <= 0 || e.brx <= e.tlx) return;
   const EventRows er = event_rows(a.s, e);
+  if constexpr (OP == OP_GRAD) {
+    grad_event(a, e, er, H, win, lane, pos);
+    return;
+  }
   constexpr int kSuper = 32 * kRowBlocks;
   LaneRows<MODE> L;
   float scale;
@@ -353,7 +403,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_tile(LaunchArgs a) {  // 2 CTAs
   __shared__ int s_next_group;
   if (threadIdx.x == 0) s_next_group = 0;
   const int lane = threadIdx.x & 31;
-  constexpr bool kReads = (OP == OP_MLEM || OP == OP_FORWARD);
+  constexpr bool kReads = (OP != OP_ADJOINT);
   constexpr bool kWrites = (OP == OP_MLEM || OP == OP_ADJOINT);
   for (int q = threadIdx.x; q < wxn * wyn; q += blockDim.x) {
     const int r = q / wxn, c = q - r * wxn;
@@ -701,6 +751,9 @@ cudaError_t launch_tile(int op, int mode, int accum, const LaunchArgs& a,
       STRIP_DISPATCH(launch_tile_t, OP_FORWARD, mode, accum, a, st);
     case OP_ADJOINT:
       STRIP_DISPATCH(launch_tile_t, OP_ADJOINT, mode, accum, a, st);
+    case OP_GRAD:  // GaussianKernel only
+      if (mode != STRIP_MODE_CPU) return cudaErrorInvalidValue;
+      return launch_tile_t<OP_GRAD, STRIP_MODE_CPU, STRIP_ACCUM_FP32>(a, st);
     default:
       return cudaErrorInvalidValue;
   }
@@ -716,6 +769,9 @@ cudaError_t launch_global(int op, int mode, int accum, const LaunchArgs& a,
       STRIP_DISPATCH(launch_global_t, OP_FORWARD, mode, accum, a, st);
     case OP_ADJOINT:
       STRIP_DISPATCH(launch_global_t, OP_ADJOINT, mode, accum, a, st);
+    case OP_GRAD:  // GaussianKernel only
+      if (mode != STRIP_MODE_CPU) return cudaErrorInvalidValue;
+      return launch_global_t<OP_GRAD, STRIP_MODE_CPU, STRIP_ACCUM_FP32>(a, st);
     default:
       return cudaErrorInvalidValue;
   }

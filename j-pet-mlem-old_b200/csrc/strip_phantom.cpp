@@ -8,6 +8,7 @@
 // uniformly over the strip acceptance instead of the reference's uniform
 // angle (phantom.h:213), and a counter-based RNG so event i is a pure
 // function of (seed, i): Philox-4x32-10 (Salmon et al., SC'11).
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -54,31 +55,14 @@ struct Region {
   }
 };
 
-}  // namespace
-
-extern "C" int strip_generate_events(const strip_geometry* g,
-                                     const strip_ellipse* el, int n_el,
-                                     uint64_t seed, int64_t n, float* z_u,
-                                     float* z_d, float* dl) {
-  if (!g || !el || n_el <= 0 || n < 0 || (n > 0 && (!z_u || !z_d || !dl)))
-    return STRIP_E_INVALID;
-  if (!(g->radius > 0) || !(g->scintillator_length > 0) ||
-      !(g->sigma_z >= 0) || !(g->sigma_dl >= 0))
-    return STRIP_E_INVALID;
-  std::vector<Region> reg((size_t)n_el);
-  std::vector<double> cdf((size_t)n_el);
-  double acc = 0;
-  for (int i = 0; i < n_el; ++i) {
-    if (!(el[i].a > 0) || !(el[i].b > 0) || !(el[i].activity >= 0))
-      return STRIP_E_INVALID;
-    const double ang = el[i].angle_deg * M_PI / 180.0;
-    reg[i] = Region{el[i].z, el[i].y, el[i].a, el[i].b, std::cos(ang),
-                    std::sin(ang), M_PI * el[i].a * el[i].b * el[i].activity};
-    acc += reg[i].w;
-    cdf[i] = acc;
-  }
-  if (!(acc > 0)) return STRIP_E_INVALID;
-  for (auto& c : cdf) c /= acc;
+// Detection and smearing shared by the generators.  `emit(c, pz, py)` fills
+// the emission point from the first three words of the attempt's Philox block
+// c and returns false when the attempt is rejected; c[3] draws tan(theta),
+// uniform over the acceptance or (uniform_angle) from an angle uniform in
+// (-pi/2, pi/2) as the reference's phantom generator (phantom.h:213).
+template <class Emit>
+int generate(const strip_geometry* g, uint64_t seed, int64_t n, float* z_u,
+             float* z_d, float* dl, const Emit& emit, bool uniform_angle = false) {
   const double R = g->radius, hL = g->scintillator_length / 2.0;
   const double tmax = g->scintillator_length / (2.0 * R);
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
@@ -93,18 +77,9 @@ extern "C" int strip_generate_events(const strip_geometry* g,
     for (uint32_t att = 0; att < (uint32_t)kMaxAttempts && !ok; ++att) {
       uint32_t c[4] = {ilo, ihi, att, 0u};
       Philox::block(c, k0, k1);
-      const double ur = u01(c[0]);
-      int r = 0;
-      while (r < n_el - 1 && ur > cdf[r]) ++r;
-      const Region& q = reg[r];
-      const double rad = std::sqrt(u01(c[1])), phi = 2.0 * M_PI * u01(c[2]);
-      const double lu = q.a * rad * std::cos(phi), lv = q.b * rad * std::sin(phi);
-      pz = q.z + lu * q.c - lv * q.s;
-      py = q.y + lu * q.s + lv * q.c;
-      bool covered = false;
-      for (int j = 0; j < r && !covered; ++j) covered = reg[j].contains(pz, py);
-      if (covered) continue;
-      t = tmax * (2.0 * u01(c[3]) - 1.0);
+      if (!emit(c, pz, py)) continue;
+      t = uniform_angle ? std::tan(M_PI * (u01(c[3]) - 0.5))
+                        : tmax * (2.0 * u01(c[3]) - 1.0);
       const double zu = pz + (R - py) * t, zd = pz - (R + py) * t;
       ok = std::fabs(zu) < hL && std::fabs(zd) < hL;
     }
@@ -126,4 +101,83 @@ extern "C" int strip_generate_events(const strip_geometry* g,
     dl[i] = (float)(d + g->sigma_dl * n2);
   }
   return bad ? STRIP_E_INVALID : STRIP_OK;
+}
+
+bool valid_geometry(const strip_geometry* g) {
+  return g && g->radius > 0 && g->scintillator_length > 0 && g->sigma_z >= 0 &&
+         g->sigma_dl >= 0;
+}
+
+}  // namespace
+
+extern "C" int strip_generate_events(const strip_geometry* g,
+                                     const strip_ellipse* el, int n_el,
+                                     uint64_t seed, int64_t n, float* z_u,
+                                     float* z_d, float* dl) {
+  if (!valid_geometry(g) || !el || n_el <= 0 || n < 0 ||
+      (n > 0 && (!z_u || !z_d || !dl)))
+    return STRIP_E_INVALID;
+  std::vector<Region> reg((size_t)n_el);
+  std::vector<double> cdf((size_t)n_el);
+  double acc = 0;
+  for (int i = 0; i < n_el; ++i) {
+    if (!(el[i].a > 0) || !(el[i].b > 0) || !(el[i].activity >= 0))
+      return STRIP_E_INVALID;
+    const double ang = el[i].angle_deg * M_PI / 180.0;
+    reg[i] = Region{el[i].z, el[i].y, el[i].a, el[i].b, std::cos(ang),
+                    std::sin(ang), M_PI * el[i].a * el[i].b * el[i].activity};
+    acc += reg[i].w;
+    cdf[i] = acc;
+  }
+  if (!(acc > 0)) return STRIP_E_INVALID;
+  for (auto& c : cdf) c /= acc;
+  return generate(g, seed, n, z_u, z_d, dl,
+                  [&](const uint32_t* c, double& pz, double& py) {
+                    const double ur = u01(c[0]);
+                    int r = 0;
+                    while (r < n_el - 1 && ur > cdf[r]) ++r;
+                    const Region& q = reg[r];
+                    const double rad = std::sqrt(u01(c[1])), phi = 2.0 * M_PI * u01(c[2]);
+                    const double lu = q.a * rad * std::cos(phi), lv = q.b * rad * std::sin(phi);
+                    pz = q.z + lu * q.c - lv * q.s;
+                    py = q.y + lu * q.s + lv * q.c;
+                    for (int j = 0; j < r; ++j)
+                      if (reg[j].contains(pz, py)) return false;
+                    return true;
+                  });
+}
+
+extern "C" int strip_generate_events_image(const strip_geometry* g,
+                                           const float* rho, uint64_t seed,
+                                           int64_t n, int uniform_angle,
+                                           float* z_u, float* z_d, float* dl) {
+  if (!valid_geometry(g) || !rho || g->n_y_pixels <= 0 || g->n_z_pixels <= 0 ||
+      !(g->pixel_height > 0) || !(g->pixel_width > 0) || n < 0 ||
+      (n > 0 && (!z_u || !z_d || !dl)))
+    return STRIP_E_INVALID;
+  const int64_t np = (int64_t)g->n_y_pixels * g->n_z_pixels;
+  std::vector<double> cdf((size_t)np);
+  double acc = 0;
+  for (int64_t j = 0; j < np; ++j) {
+    if (!(rho[j] >= 0) || !std::isfinite(rho[j])) return STRIP_E_INVALID;
+    acc += rho[j];
+    cdf[(size_t)j] = acc;
+  }
+  if (!(acc > 0)) return STRIP_E_INVALID;
+  for (auto& c : cdf) c /= acc;
+  const double tl_y = g->center_y + g->n_y_pixels * g->pixel_height / 2.0;
+  const double tl_z = g->center_z - g->n_z_pixels * g->pixel_width / 2.0;
+  const int nz = g->n_z_pixels;
+  return generate(g, seed, n, z_u, z_d, dl,
+                  [&](const uint32_t* c, double& pz, double& py) {
+                    const double ur = u01(c[0]);
+                    int64_t j = std::lower_bound(cdf.begin(), cdf.end(), ur) - cdf.begin();
+                    if (j >= np) j = np - 1;
+                    while (rho[j] <= 0) --j;  // ur rounded past the end: last non-empty pixel
+                    const int64_t iy = j / nz, iz = j - iy * nz;
+                    pz = tl_z + ((double)iz + u01(c[1])) * g->pixel_width;
+                    py = tl_y - ((double)iy + u01(c[2])) * g->pixel_height;
+                    return true;
+                  },
+                  uniform_angle != 0);
 }

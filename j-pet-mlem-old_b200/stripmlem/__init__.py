@@ -112,6 +112,8 @@ class Reconstruction:
         if rc != STRIP_OK:
             raise StripError(rc, "strip_ctx_create")
         self._ctx = ctx
+        self.device = int(device)
+        self.torch_device = f"cuda:{self.device}"
         self.n_events = 0
         self.n_subsets = 1
         self._check(self.lib.strip_set_accumulation(self._ctx, accumulation))
@@ -228,6 +230,34 @@ class Reconstruction:
 
     iterate = __call__
 
+    # -- split iteration (events sharded over processes) -------------------
+    def set_accumulator(self, acc):
+        """Makes ``acc`` (a float64 CUDA tensor of n_y * n_z values on this
+        context's device) the backprojection accumulator and zero-fills it;
+        None returns to the context's own buffer."""
+        if acc is None:
+            self._check(self.lib.strip_set_accumulator(self._ctx, None))
+            self._acc = None
+            return
+        if (acc.dtype.itemsize != 8 or not acc.is_cuda or not acc.is_contiguous()
+                or acc.numel() != self.scanner.total_n_pixels):
+            raise StripError(_lib.STRIP_E_INVALID,
+                             "accumulator must be a contiguous float64 CUDA tensor "
+                             "of n_y * n_z values")
+        self._check(self.lib.strip_set_accumulator(self._ctx, acc.data_ptr()))
+        self._acc = acc  # keeps the buffer alive while the context uses it
+
+    def accumulate(self, subset=0, n_subsets=1, mode=None):
+        """acc_j += sum over the subset's events of P_ej / D_e (no update)."""
+        mode = self.mode if mode is None else mode
+        self._check(self.lib.strip_accumulate(self._ctx, int(mode), int(n_subsets),
+                                              int(subset)))
+        self.n_subsets = int(n_subsets)
+
+    def update(self, scale=1.0):
+        """rho_j <- rho_j * acc_j * scale; acc_j <- 0."""
+        self._check(self.lib.strip_update(self._ctx, float(scale)))
+
     # -- projections ------------------------------------------------------
     def forward(self, rho, sigma_z=None, sigma_dl=None, mode=None):
         sz = self.scanner.sigma_z if sigma_z is None else float(sigma_z)
@@ -293,6 +323,26 @@ def generate_events(scanner, ellipses, n, seed=1):
                                    _fp(zu), _fp(zd), _fp(dl))
     if rc != STRIP_OK:
         raise StripError(rc, "strip_generate_events")
+    return zu, zd, dl
+
+
+def generate_events_image(scanner, rho, n, seed=1, uniform_angle=False):
+    """Seeded synthetic events emitted from an activity image
+    (strip_generate_events_image); returns z_u, z_d, dl.  ``uniform_angle``
+    draws the emission angle uniformly (the strip kernel's model) instead of
+    tan(theta) uniformly over the acceptance."""
+    lib = _lib.load()
+    img = np.ascontiguousarray(rho, dtype=np.float32)
+    if img.size != scanner.n_y_pixels * scanner.n_z_pixels:
+        raise ValueError("rho must hold n_y_pixels * n_z_pixels values")
+    zu = np.empty(n, np.float32)
+    zd = np.empty(n, np.float32)
+    dl = np.empty(n, np.float32)
+    g = scanner.geometry()
+    rc = lib.strip_generate_events_image(ctypes.byref(g), _fp(img), int(seed), int(n),
+                                         int(bool(uniform_angle)), _fp(zu), _fp(zd), _fp(dl))
+    if rc != STRIP_OK:
+        raise StripError(rc, "strip_generate_events_image")
     return zu, zd, dl
 
 

@@ -110,11 +110,27 @@ SIGNATURES = {
         ctypes.c_int,
         [_ctx, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, PROGRESS_CB, ctypes.c_void_p],
     ),
+    "strip_set_accumulator": (ctypes.c_int, [_ctx, ctypes.c_void_p]),
+    "strip_accumulate": (ctypes.c_int, [_ctx, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "strip_update": (ctypes.c_int, [_ctx, ctypes.c_double]),
     "strip_forward": (ctypes.c_int, [_ctx, _f, ctypes.c_double, ctypes.c_double, ctypes.c_int, _d]),
     "strip_adjoint": (ctypes.c_int, [_ctx, _d, ctypes.c_double, ctypes.c_double, ctypes.c_int, _d]),
     "strip_grad_sigma": (
         ctypes.c_int,
         [_ctx, _f, _d, ctypes.c_double, ctypes.c_double, _d, _d],
+    ),
+    "strip_forward_device": (
+        ctypes.c_int,
+        [_ctx, ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_void_p],
+    ),
+    "strip_adjoint_device": (
+        ctypes.c_int,
+        [_ctx, ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_void_p],
+    ),
+    "strip_grad_sigma_device": (
+        ctypes.c_int,
+        [_ctx, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+         ctypes.c_void_p],
     ),
     "strip_debug_pixel_sets": (
         ctypes.c_int,
@@ -133,6 +149,10 @@ SIGNATURES = {
     "strip_generate_events": (
         ctypes.c_int,
         [_P(Geometry), _P(Ellipse), ctypes.c_int, ctypes.c_uint64, ctypes.c_int64, _f, _f, _f],
+    ),
+    "strip_generate_events_image": (
+        ctypes.c_int,
+        [_P(Geometry), _f, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int, _f, _f, _f],
     ),
 }
 
