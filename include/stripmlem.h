@@ -135,7 +135,9 @@ int strip_set_events_device(strip_ctx* ctx, const float* d_z_u,
 
 /* ---- image -------------------------------------------------------------- */
 
-/* rho in / out (host, n_y * n_z floats); Reconstruction::rho / run()'s rho_io. */
+/* rho in / out (host, n_y * n_z floats); Reconstruction::rho / run()'s rho_io.
+ * An activity image is non-negative and finite: strip_set_image rejects
+ * anything else with STRIP_E_INVALID (the reference does not check). */
 int strip_set_image(strip_ctx* ctx, const float* rho);
 int strip_get_image(strip_ctx* ctx, float* rho);
 /* Sensitivity image: five_point = 1 gives Scanner::pixel_sensitivity

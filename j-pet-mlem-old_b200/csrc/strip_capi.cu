@@ -34,6 +34,7 @@ struct strip_ctx {
   float* d_rho = nullptr;
   double* d_acc = nullptr;      // accumulator in use (own or the caller's)
   double* d_acc_own = nullptr;  // the context's own accumulator
+  int acc_mode = STRIP_MODE_CPU;  // mode of the last strip_accumulate
   float* d_sens5 = nullptr;
   // binned events
   int64_t n_events = 0;   // as given by the caller
@@ -126,6 +127,8 @@ KernelF make_kernel(double sigma_z, double sigma_dl, float pw) {
   k.r1 = 2.0f * k.c1 * pw;
   k.r0 = k.c1 * pw * pw;
   k.q = (float)exp2(2.0 * (double)k.c1 * (double)pw * (double)pw);
+  k.q3 = (float)exp2(6.0 * (double)k.c1 * (double)pw * (double)pw);
+  k.q4 = (float)exp2(8.0 * (double)k.c1 * (double)pw * (double)pw);
   k.lg2kc = (float)log2((double)k.kc);
   return k;
 }
@@ -268,25 +271,31 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
   CKB(launch_bin_scatter(keys, n, zu, zd, dl, orig, d_hist, ozu, ozd, odl,
                          operm, st));
 
-  // Work items: chunks of each (subset, tile) bin, sized for >= ~8 waves.
+  // Work items: chunks of each (subset, tile) bin, sized for >= ~8 waves and
+  // at most kMaxItemEvents events (the fixed-point window accumulator's
+  // bound).  Chunk k of every tile precedes chunk k + 1 of any tile, so the
+  // CTAs resident at one time work on different tiles and their window
+  // flushes rarely hit the same pixels together.
   std::vector<WorkItem> items;
   std::vector<int> ib(n_subsets), ic(n_subsets);
   std::vector<int64_t> gb(n_subsets), gc(n_subsets);
   const int64_t per_sub = (int64_t)(total / (unsigned long long)n_subsets) + 1;
   const int64_t target = (int64_t)ctx->sm_count * 2 * 8;
-  const int64_t chunk =
-      std::min<int64_t>(1 << 15, std::max<int64_t>(2048, per_sub / target + 1));
+  const int64_t chunk = std::min<int64_t>(
+      kMaxItemEvents, std::max<int64_t>(2048, per_sub / target + 1));
   for (int sb = 0; sb < n_subsets; ++sb) {
     ib[sb] = (int)items.size();
-    for (int tile = 0; tile < t.n_tiles; ++tile) {
-      const int key = sb * (t.n_tiles + 1) + tile;
-      int64_t b = (int64_t)offs[key], c = (int64_t)hist[key];
-      while (c > 0) {
+    for (int64_t round = 0;; ++round) {
+      bool any = false;
+      for (int tile = 0; tile < t.n_tiles; ++tile) {
+        const int key = sb * (t.n_tiles + 1) + tile;
+        const int64_t c = (int64_t)hist[key] - round * chunk;
+        if (c <= 0) continue;
         const int64_t m = std::min(c, chunk);
-        items.push_back(WorkItem{tile, (int32_t)m, b});
-        b += m;
-        c -= m;
+        items.push_back(WorkItem{tile, (int32_t)m, (int64_t)offs[key] + round * chunk});
+        any = true;
       }
+      if (!any) break;
     }
     ic[sb] = (int)items.size() - ib[sb];
     const int gkey = sb * (t.n_tiles + 1) + t.n_tiles;
@@ -589,6 +598,11 @@ int strip_set_responses(strip_ctx* ctx, const float* t, int64_t n,
 
 int strip_set_image(strip_ctx* ctx, const float* rho) {
   if (!ctx || !rho) return STRIP_E_INVALID;
+  for (int64_t j = 0; j < ctx->n_pix; ++j)
+    if (!(rho[j] >= 0.0f) || !std::isfinite(rho[j]))
+      return fail(ctx, STRIP_E_INVALID,
+                  "strip_set_image: pixel %lld is negative or not finite",
+                  (long long)j);
   if (int rc = set_device(ctx)) return rc;
   CK(cudaMemcpyAsync(ctx->d_rho, rho, ctx->n_pix * sizeof(float),
                      cudaMemcpyHostToDevice, ctx->stream));
@@ -658,7 +672,7 @@ int strip_iterate(strip_ctx* ctx, int n_iter, int mode, int n_subsets,
       ++mark;
       CK(launch_global(OP_MLEM, mode, ctx->accum, a, ctx->stream));
       CK(launch_update(ctx->d_rho, ctx->d_acc, ctx->n_pix,
-                       (double)ctx->n_subsets, ctx->stream));
+                       (double)ctx->n_subsets, mlem_weighted(mode), ctx->stream));
       launches += (a.n_items > 0) + (a.g_count > 0) + 1;
     }
     if (progress) {
@@ -730,6 +744,7 @@ int strip_accumulate(strip_ctx* ctx, int mode, int n_subsets, int subset) {
   ctx->stats.last_iterate_ms = ms;
   ctx->stats.last_tile_ms = ms;
   ctx->stats.kernel_launches = (a.n_items > 0) + (a.g_count > 0);
+  ctx->acc_mode = mode;
   return STRIP_OK;
 }
 
@@ -738,7 +753,8 @@ int strip_update(strip_ctx* ctx, double scale) {
   if (!(scale > 0) || !std::isfinite(scale))
     return fail(ctx, STRIP_E_INVALID, "invalid update scale");
   if (int rc = set_device(ctx)) return rc;
-  CK(launch_update(ctx->d_rho, ctx->d_acc, ctx->n_pix, scale, ctx->stream));
+  CK(launch_update(ctx->d_rho, ctx->d_acc, ctx->n_pix, scale,
+                   mlem_weighted(ctx->acc_mode), ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return STRIP_OK;
 }

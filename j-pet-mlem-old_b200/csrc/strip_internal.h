@@ -20,6 +20,26 @@ struct WorkItem {
   int64_t begin;
 };
 
+// MLEM backprojection with the reference CPU semantics accumulates, per event
+// and pixel, u = K_j rho_j / D_e -- what reconstruction.h:276-295 scatters --
+// and u lies in [0, 1] because D_e = sum_k K_k rho_k.  The tile kernel's
+// shared-memory window therefore accumulates u in unsigned 32-bit fixed point
+// (native integer shared atomics instead of a compare-and-swap loop per
+// binary32 add).  A work item of `count` events uses the scale 2^s with the
+// largest s <= kMaxFixedShift for which (count + count/128 + 1) * 2^s <=
+// 2^32, so no pixel sum can wrap: s = 19 for the largest items
+// (kMaxItemEvents), 22 for 1016 events, 30 for the smallest.
+constexpr int kMaxFixedShift = 30;
+constexpr int kMaxItemEvents = 8000;
+
+__host__ __device__ inline int fixed_shift(int count) {
+  const unsigned m = (unsigned)count + ((unsigned)count >> 7) + 1u;
+  int lg = 0;  // ceil(log2(m))
+  while ((1u << lg) < m && lg < 31) ++lg;
+  const int s = 32 - lg;
+  return s < kMaxFixedShift ? s : kMaxFixedShift;
+}
+
 // Image tiling.  Tile (bx, by) owns pixels [bx*TX, (bx+1)*TX) x [by*TY, ...);
 // its shared-memory window adds a halo of (HX, HY) pixels on each side,
 // clamped to the image.  WXmax/WYmax bound every window, WS is the padded
@@ -104,12 +124,16 @@ cudaError_t launch_tile(int op, int mode, int accum, const LaunchArgs& a,
                         cudaStream_t st);
 cudaError_t launch_global(int op, int mode, int accum, const LaunchArgs& a,
                           cudaStream_t st);
+// rho_j <- rho_j * acc_j * scale, or acc_j * scale when the accumulator holds
+// rho-weighted contributions (weighted: STRIP_MODE_CPU MLEM); acc_j <- 0.
 cudaError_t launch_update(float* rho, double* acc, int64_t n_pix, double scale,
-                          cudaStream_t st);
-// rho_out_j = rho_in_j * acc_j (acc is left as is)
+                          int weighted, cudaStream_t st);
+// rho_out_j = rho_in_j * acc_j, or acc_j when weighted (acc is left as is)
 cudaError_t launch_update_out(const float* rho_in, float* rho_out,
-                              const double* acc, int64_t n_pix,
+                              const double* acc, int64_t n_pix, int weighted,
                               cudaStream_t st);
+// Whether MLEM in `mode` accumulates rho-weighted contributions.
+inline int mlem_weighted(int mode) { return mode == STRIP_MODE_CPU; }
 cudaError_t launch_sensitivity(const ScannerF& s, int five_point, float* out,
                                cudaStream_t st);
 cudaError_t launch_debug_sets(const ScannerF& s, const float* zu,

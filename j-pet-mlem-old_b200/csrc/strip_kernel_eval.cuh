@@ -38,6 +38,30 @@ __device__ __forceinline__ float rcp_approx(float x) {
 
 constexpr float kLog2e = 1.4426950408889634f;
 
+// Packed binary32 pairs: sm_100's f32x2 arithmetic issues one instruction for
+// two multiplies or FMAs (each lane rounded like its scalar form).
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pack2(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ float2 unpack2(f32x2 v) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+  return r;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
 // Kernel constants for given sigmas (the sigmas of the model, which may differ
 // from the geometry's sigmas that fix the pixel sets).
 struct KernelF {
@@ -47,7 +71,26 @@ struct KernelF {
   //   E(t + pw) = E(t) * R(t),  R(t) = 2^(r1 t + r0),  R(t + pw) = R(t) * q
   float r1, r0;  // 2 c1 pw, c1 pw^2
   float q;       // 2^(2 c1 pw^2)
+  float q3, q4;  // q^3, q^4: the pixel-pair form of the recurrence
   float lg2kc;   // log2(kc)
+};
+
+// The Gaussian along a run, two pixels per step: with R_k = R_0 q^k,
+//   (E_2i+2, E_2i+3) = (E_2i, E_2i+1) * S_i,  S_i = (R_2i R_2i+1, R_2i+1 R_2i+2),
+//   S_i+1 = S_i * q^4,  S_0 = (R_0^2 q, R_0^2 q^3).
+struct PairRecurrence {
+  f32x2 P, S, Q4;
+  __device__ __forceinline__ PairRecurrence(const KernelF& k, float E0,
+                                            float R0) {
+    const float R2 = R0 * R0;
+    P = pack2(E0, E0 * R0);
+    S = pack2(R2 * k.q, R2 * k.q3);
+    Q4 = pack2(k.q4, k.q4);
+  }
+  __device__ __forceinline__ void step() {
+    P = mul2(P, S);
+    S = mul2(S, Q4);
+  }
 };
 
 // GaussianKernel, one row.

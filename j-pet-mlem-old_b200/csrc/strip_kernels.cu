@@ -86,17 +86,60 @@ struct RowSum<STRIP_ACCUM_FP64> {
   __device__ __forceinline__ double total() const { return s; }
 };
 
-// Shared-memory window of the image: w = rho (* s), acc = partial backprojection.
+// Binary32 -> unsigned integer by the 2^23 addend: for 0 <= x * s < 2^23 the
+// bits of x * s + 2^23 (one FFMA, round to nearest) minus those of 2^23 are
+// round(x * s).
+constexpr float kMagic = 8388608.0f;
+constexpr unsigned kMagicBits = 0x4B000000u;
+__device__ __forceinline__ unsigned to_fixed(float x, float s) {
+  return __float_as_uint(fmaf(x, s, kMagic)) - kMagicBits;
+}
+
+// Shared-memory window of the image: w = rho (* s), acc = partial
+// backprojection -- binary32 (acc) or, for the rho-weighted MLEM
+// accumulation, 2^kFixedShift fixed point (acc_u).
+// FINE: scales above 2^22 (items of fewer than ~1000 events) convert with
+// cvt.rni (the conversion pipe) instead of the 2^23 addend.
+template <bool FINE>
 struct SmemWin {
   const float* w;
   float* acc;
   int wx0, wy0, WS;
+  float fixed_unit;  // 2^fixed_shift(item events)
+  __device__ __forceinline__ float unit() const { return fixed_unit; }
   __device__ __forceinline__ int ptr(int iy, int col) const {
     return (iy - wy0) * WS + (col - wx0);
   }
   __device__ __forceinline__ float read(int p, int j) const { return w[p + j]; }
   __device__ __forceinline__ void add(int p, int j, float v) const {
     atomicAdd(acc + p + j, v);
+  }
+  // acc_j += K_j w_j / D_e for K_j = E * pref and sc = pref / D_e * unit()
+  __device__ __forceinline__ void add_weighted(int p, int j, float E,
+                                               float sc) const {
+    const unsigned v = FINE ? __float2uint_rn(E * w[p + j] * sc)
+                            : to_fixed(E * w[p + j], sc);
+    atomicAdd(reinterpret_cast<unsigned*>(acc) + p + j, v);
+  }
+  // the same for pixels j, j + 1 with K = P * pref (packed)
+  static constexpr bool kPairScatter = true;
+  __device__ __forceinline__ void add_weighted2(int p, int j, f32x2 P,
+                                                float sc) const {
+    unsigned* au = reinterpret_cast<unsigned*>(acc) + p + j;
+    const f32x2 kw = mul2(P, pack2(w[p + j], w[p + j + 1]));
+    unsigned v0, v1;
+    if constexpr (FINE) {
+      const float2 x = unpack2(mul2(kw, pack2(sc, sc)));
+      v0 = __float2uint_rn(x.x);
+      v1 = __float2uint_rn(x.y);
+    } else {
+      const float2 x =
+          unpack2(fma2(kw, pack2(sc, sc), pack2(kMagic, kMagic)));
+      v0 = __float_as_uint(x.x) - kMagicBits;
+      v1 = __float_as_uint(x.y) - kMagicBits;
+    }
+    atomicAdd(au, v0);
+    atomicAdd(au + 1, v1);
   }
 };
 
@@ -117,6 +160,12 @@ struct GlobalWin {
   }
   __device__ __forceinline__ void add(int64_t p, int j, float v) const {
     atomicAdd(acc + p + j, (double)v);
+  }
+  __device__ __forceinline__ float unit() const { return 1.0f; }
+  static constexpr bool kPairScatter = false;
+  __device__ __forceinline__ void add_weighted(int64_t p, int j, float E,
+                                               float sc) const {
+    atomicAdd(acc + p + j, (double)(E * read(p, j) * sc));
   }
 };
 
@@ -152,6 +201,11 @@ __device__ __forceinline__ void walk_share(const RowTables& T, int nrows,
 // rebuilt for pass 2.
 // ---------------------------------------------------------------------------
 constexpr int kRowBlocks = 3;
+// Walk GaussianKernel runs two pixels per step with packed f32x2 arithmetic.
+#ifndef STRIP_PAIRS
+#define STRIP_PAIRS 1
+#endif
+constexpr bool kPairs = STRIP_PAIRS != 0;
 
 __device__ __forceinline__ int ranked_row(int H, int i) {
   const int mid = (H - 1) >> 1;
@@ -235,7 +289,19 @@ __device__ __forceinline__ void pass1_rows(const ScannerF& s, const KernelF& k,
       const auto p = win.ptr(e.tly + ranked_row(H, rank0 + 32 * b + lane),
                              run_lo(L.lolen[b]));
       float a = 0.0f;
-      if constexpr (MODE == STRIP_MODE_CPU) {
+      if constexpr (MODE == STRIP_MODE_CPU && kPairs) {
+        PairRecurrence g(k, L.E0[b], L.R0[b]);
+        f32x2 A = pack2(0.0f, 0.0f);
+#pragma unroll 2
+        for (int j = 0; j + 1 < n; j += 2) {
+          A = fma2(g.P, pack2(win.read(p, j), win.read(p, j + 1)), A);
+          g.step();
+        }
+        const float2 a2 = unpack2(A);
+        a = a2.x + a2.y;
+        if (n & 1) a = fmaf(unpack2(g.P).x, win.read(p, n - 1), a);
+        acc.add(L.pref[b] * a);
+      } else if constexpr (MODE == STRIP_MODE_CPU) {
         float E = L.E0[b], R = L.R0[b];
 #pragma unroll 4
         for (int j = 0; j < n; ++j) {
@@ -260,8 +326,9 @@ __device__ __forceinline__ void pass1_rows(const ScannerF& s, const KernelF& k,
   }
 }
 
-// Pass 2 over the lane's rows: acc_j += K_j * scale.
-template <int MODE, class Win>
+// Pass 2 over the lane's rows: acc_j += K_j * scale, or, WEIGHTED (MLEM with
+// the reference CPU semantics), acc_j += K_j * w_j * scale.
+template <int MODE, bool WEIGHTED, class Win>
 __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
                                            const EventF& e, int H, int rank0,
                                            int lane, const LaneRows<MODE>& L,
@@ -273,7 +340,26 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
     if (b < nb && n > 0) {
       const auto p = win.ptr(e.tly + ranked_row(H, rank0 + 32 * b + lane),
                              run_lo(L.lolen[b]));
-      if constexpr (MODE == STRIP_MODE_CPU) {
+      if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED && kPairs &&
+                    Win::kPairScatter) {
+        PairRecurrence g(k, L.E0[b], L.R0[b]);
+        const float sc = fminf(L.pref[b] * scale * win.unit(), 3.0e38f);
+#pragma unroll 2
+        for (int j = 0; j + 1 < n; j += 2) {
+          win.add_weighted2(p, j, g.P, sc);
+          g.step();
+        }
+        if (n & 1) win.add_weighted(p, n - 1, unpack2(g.P).x, sc);
+      } else if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED) {
+        float E = L.E0[b], R = L.R0[b];
+        const float sc = fminf(L.pref[b] * scale * win.unit(), 3.0e38f);
+#pragma unroll 4
+        for (int j = 0; j < n; ++j) {
+          win.add_weighted(p, j, E, sc);
+          E *= R;
+          R *= k.q;
+        }
+      } else if constexpr (MODE == STRIP_MODE_CPU) {
         float E = L.E0[b], R = L.R0[b];
         const float sc = L.pref[b] * scale;
 #pragma unroll 4
@@ -376,19 +462,47 @@ __device__ __forceinline__ void process_event(const LaunchArgs& a,
     scale = (float)a.w_in[a.perm[pos]];
     if (scale == 0.0f) return;
   }
+  constexpr bool kWeighted = OP == OP_MLEM && MODE == STRIP_MODE_CPU;
   if ((OP == OP_MLEM) && H <= kSuper) {
-    pass2_rows<MODE>(a.s, a.k, e, H, 0, lane, L, (H + 31) >> 5, win, scale);
+    pass2_rows<MODE, kWeighted>(a.s, a.k, e, H, 0, lane, L, (H + 31) >> 5, win,
+                                scale);
     return;
   }
   for (int r0 = 0; r0 < H; r0 += kSuper) {
     build_lane_rows<MODE>(a.s, a.k, e, er, H, r0, lane, L);
-    pass2_rows<MODE>(a.s, a.k, e, H, r0, lane, L,
-                     min(kRowBlocks, (H - r0 + 31) >> 5), win, scale);
+    pass2_rows<MODE, kWeighted>(a.s, a.k, e, H, r0, lane, L,
+                                min(kRowBlocks, (H - r0 + 31) >> 5), win, scale);
   }
 }
 
 __device__ __forceinline__ RowTables warp_tables(char* base, int cap, int warp) {
   return row_tables_at(base + (size_t)warp * row_table_bytes(cap), cap);
+}
+
+// The events of a work item: warps pull groups of kGrab events from a shared
+// counter until the item is done (lanes < kGrab set the group's events up in
+// parallel).
+template <int OP, int MODE, int ACC, class Win>
+__device__ __forceinline__ void run_item(const LaunchArgs& a, const WorkItem& it,
+                                         const Win& win, int lane,
+                                         int* next_group) {
+  const int64_t end = it.begin + it.count;
+  for (;;) {
+    int g = 0;
+    if (lane == 0) g = atomicAdd(next_group, 1);
+    g = __shfl_sync(kFull, g, 0);
+    const int64_t base = it.begin + (int64_t)g * kGrab;
+    if (base >= end) break;
+    const int64_t ei = base + lane;
+    EventF mine = {};
+    if (lane < kGrab && ei < end)
+      event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], mine);
+    const int nh = (int)min((int64_t)kGrab, end - base);
+    for (int j = 0; j < nh; ++j) {
+      const EventF e = shfl_event(mine, j);
+      process_event<OP, MODE, ACC>(a, e, win, lane, base + j);
+    }
+  }
 }
 
 template <int OP, int MODE, int ACC>
@@ -416,33 +530,27 @@ __global__ void __launch_bounds__(kThreads, 2) k_tile(LaunchArgs a) {  // 2 CTAs
     if (kWrites) s_acc[r * WS + c] = 0.0f;
   }
   __syncthreads();
-  const SmemWin win{s_w, s_acc, wx0, wy0, WS};
-  const int64_t end = it.begin + it.count;
-  // warps pull groups of kGrab events from a shared counter until the item is
-  // done (lanes < kGrab set the group's events up in parallel)
-  for (;;) {
-    int g = 0;
-    if (lane == 0) g = atomicAdd(&s_next_group, 1);
-    g = __shfl_sync(kFull, g, 0);
-    const int64_t base = it.begin + (int64_t)g * kGrab;
-    if (base >= end) break;
-    const int64_t ei = base + lane;
-    EventF mine = {};
-    if (lane < kGrab && ei < end)
-      event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], mine);
-    const int nh = (int)min((int64_t)kGrab, end - base);
-    for (int j = 0; j < nh; ++j) {
-      const EventF e = shfl_event(mine, j);
-      process_event<OP, MODE, ACC>(a, e, win, lane, base + j);
-    }
-  }
+  const int fshift = fixed_shift(it.count);
+  const float unit = (float)(1u << fshift);
+  if (fshift > 22)
+    run_item<OP, MODE, ACC>(a, it, SmemWin<true>{s_w, s_acc, wx0, wy0, WS, unit},
+                            lane, &s_next_group);
+  else
+    run_item<OP, MODE, ACC>(a, it, SmemWin<false>{s_w, s_acc, wx0, wy0, WS, unit},
+                            lane, &s_next_group);
   if (kWrites) {
     __syncthreads();
+    constexpr bool kFixed = OP == OP_MLEM && MODE == STRIP_MODE_CPU;
+    const unsigned* s_acc_u = reinterpret_cast<const unsigned*>(s_acc);
     for (int q = threadIdx.x; q < wxn * wyn; q += blockDim.x) {
       const int r = q / wxn, c = q - r * wxn;
-      const float v = s_acc[r * WS + c];
-      if (v != 0.0f)
-        atomicAdd(a.acc + (int64_t)(wy0 + r) * a.s.n_z + wx0 + c, (double)v);
+      double v;
+      if constexpr (kFixed)
+        v = ldexp((double)s_acc_u[r * WS + c], -fshift);
+      else
+        v = (double)s_acc[r * WS + c];
+      if (v != 0.0)
+        atomicAdd(a.acc + (int64_t)(wy0 + r) * a.s.n_z + wx0 + c, v);
     }
   }
 }
@@ -555,16 +663,18 @@ __global__ void k_bin_scatter(const int* keys, int64_t n, const float* zu,
 }
 
 __global__ void k_update_out(const float* rho_in, float* rho_out,
-                             const double* acc, int64_t n) {
+                             const double* acc, int64_t n, int weighted) {
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
        j += (int64_t)gridDim.x * blockDim.x)
-    rho_out[j] = (float)((double)rho_in[j] * acc[j]);
+    rho_out[j] = weighted ? (float)acc[j] : (float)((double)rho_in[j] * acc[j]);
 }
 
-__global__ void k_update(float* rho, double* acc, int64_t n, double scale) {
+__global__ void k_update(float* rho, double* acc, int64_t n, double scale,
+                         int weighted) {
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
        j += (int64_t)gridDim.x * blockDim.x) {
-    rho[j] = (float)((double)rho[j] * acc[j] * scale);
+    rho[j] = weighted ? (float)(acc[j] * scale)
+                      : (float)((double)rho[j] * acc[j] * scale);
     acc[j] = 0.0;
   }
 }
@@ -809,15 +919,17 @@ cudaError_t launch_bin_scatter(const int* keys, int64_t n, const float* zu,
 }
 
 cudaError_t launch_update(float* rho, double* acc, int64_t n_pix, double scale,
-                          cudaStream_t st) {
-  k_update<<<grid_for(n_pix), kThreads, 0, st>>>(rho, acc, n_pix, scale);
+                          int weighted, cudaStream_t st) {
+  k_update<<<grid_for(n_pix), kThreads, 0, st>>>(rho, acc, n_pix, scale,
+                                                 weighted);
   return cudaGetLastError();
 }
 
 cudaError_t launch_update_out(const float* rho_in, float* rho_out,
-                              const double* acc, int64_t n_pix,
+                              const double* acc, int64_t n_pix, int weighted,
                               cudaStream_t st) {
-  k_update_out<<<grid_for(n_pix), kThreads, 0, st>>>(rho_in, rho_out, acc, n_pix);
+  k_update_out<<<grid_for(n_pix), kThreads, 0, st>>>(rho_in, rho_out, acc, n_pix,
+                                                     weighted);
   return cudaGetLastError();
 }
 

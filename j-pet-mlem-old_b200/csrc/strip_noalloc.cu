@@ -104,7 +104,7 @@ extern "C" int strip_iterate_noalloc(const strip_geometry* g, const float* d_z_u
     e = launch_sensitivity(a.s, 1, sens, st);
   if (e == cudaSuccess)
     e = launch_global(OP_MLEM, mode, STRIP_ACCUM_KAHAN, a, st);
-  if (e == cudaSuccess) e = launch_update_out(d_rho_in, d_rho_out, acc, n_pix, st);
+  if (e == cudaSuccess) e = launch_update_out(d_rho_in, d_rho_out, acc, n_pix, mlem_weighted(mode), st);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return e == cudaErrorMemoryAllocation ? STRIP_E_NOMEM : STRIP_E_CUDA;

@@ -137,28 +137,34 @@ def log_likelihood(rec_data, rec_norm, cell_volume, rho, sigma, weights=None):
     return data - n * torch.log(cell_volume * yq.sum())
 
 
-def fit_sigma(rec_data, rec_norm, cell_volume, rho, sigma0, steps=60, lr=0.05,
+def fit_sigma(rec_data, rec_norm, cell_volume, rho, sigma0, max_iter=60,
               weights=None, callback=None):
-    """Fits (sigma_z, sigma_dl) from sigma0 by Adam on log sigma (learning
-    rate annealed from lr to lr / 50 on a cosine), maximising
-    log_likelihood().  Returns (sigma, history of (l, sigma_z, sigma_dl)).
-    rec_data holds the events, rec_norm the quadrature events."""
+    """Fits (sigma_z, sigma_dl) from sigma0, maximising log_likelihood() by
+    L-BFGS with a strong-Wolfe line search on log sigma (two parameters, a
+    smooth objective).  Returns (sigma, history of (l, sigma_z, sigma_dl) per
+    objective evaluation).  rec_data holds the events, rec_norm the
+    quadrature events."""
     logs = torch.tensor([math.log(sigma0[0]), math.log(sigma0[1])], dtype=torch.float64,
                         requires_grad=True)
-    opt = torch.optim.Adam([logs], lr=lr)
-    sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, T_max=steps, eta_min=lr / 50)
+    opt = torch.optim.LBFGS([logs], lr=1.0, max_iter=max_iter, tolerance_grad=1e-9,
+                            tolerance_change=1e-12, history_size=10,
+                            line_search_fn="strong_wolfe")
+    scale = 1.0 / max(1, rec_data.n_events)
     hist = []
-    for it in range(steps):
+
+    def closure():
         opt.zero_grad()
         sigma = torch.exp(logs)
         ll = log_likelihood(rec_data, rec_norm, cell_volume, rho, sigma, weights)
-        (-ll / max(1, rec_data.n_events)).backward()
-        opt.step()
-        sched.step()
-        s = torch.exp(logs).detach()
+        loss = -ll * scale
+        loss.backward()
+        s = sigma.detach()
         hist.append((float(ll.detach()), float(s[0]), float(s[1])))
         if callback is not None:
-            callback(it, hist[-1])
+            callback(len(hist) - 1, hist[-1])
+        return loss
+
+    opt.step(closure)
     return torch.exp(logs).detach(), hist
 
 

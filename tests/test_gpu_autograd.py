@@ -29,7 +29,12 @@ def case():
     ev = sm.generate_events(sc, C1_PHANTOM, n, seed=32)
     rng = np.random.default_rng(7)
     rho = rng.lognormal(0.0, 0.5, size=(g.n_y_pixels, g.n_z_pixels)).astype(np.float32)
-    w = rng.uniform(0.5, 1.5, size=n)
+    # weights that make d(w'y)/dsigma large: the kernel integrates to nearly
+    # the same total at every sigma, so uniform weights would leave only a
+    # small residual (and a cancellation-dominated test); w ~ y weighs the
+    # kernel cores, whose height falls as sigma grows
+    y0 = orc.forward_f64(g, *ev, rho, C1["s_z"], C1["s_dl"])
+    w = y0 / y0.mean() * rng.uniform(0.9, 1.1, size=n)
     return sc, g, ev, rho, w
 
 
@@ -55,11 +60,15 @@ def test_grad_sigma_vs_central_differences_of_the_kernels(case):
 
         def f(a, b):
             return float(np.dot(w, rec.forward(rho, a, b, mode=0)))
-        hz, hd = 2e-3 * sz, 2e-3 * sdl
+        # binary32 forward values carry ~1e-7 relative noise (ex2.approx,
+        # rounding), so the step is 1 % of sigma and the bar 0.5 %; the FP64
+        # oracle's gradient meets its own differences to 1e-6
+        # (tests/test_oracle_grad.py)
+        hz, hd = 1e-2 * sz, 1e-2 * sdl
         fz = (f(sz + hz, sdl) - f(sz - hz, sdl)) / (2 * hz)
         fd = (f(sz, sdl + hd) - f(sz, sdl - hd)) / (2 * hd)
-    assert abs(gz - fz) <= 2e-3 * abs(fz)
-    assert abs(gdl - fd) <= 2e-3 * abs(fd)
+    assert abs(gz - fz) <= 5e-3 * abs(fz)
+    assert abs(gdl - fd) <= 5e-3 * abs(fd)
 
 
 @pytest.mark.parametrize("mode", [0, 1])
@@ -118,6 +127,5 @@ def test_sigma_fit_recovers_the_model_sigmas():
         rq.set_events(qu, qd, ql)
         with torch.no_grad():
             yq = sa.project(rq, rho_t, torch.tensor([8.0, 30.0], dtype=torch.float64), 0)
-        s, hist = sa.fit_sigma(rq, rq, vol, rho_t, (15.0, 60.0), steps=80, lr=0.05,
-                               weights=vol * yq)
-    assert abs(float(s[0]) - 8.0) < 0.08 and abs(float(s[1]) - 30.0) < 0.3, hist[-5:]
+        s, hist = sa.fit_sigma(rq, rq, vol, rho_t, (15.0, 60.0), weights=vol * yq)
+    assert abs(float(s[0]) - 8.0) < 0.04 and abs(float(s[1]) - 30.0) < 0.15, hist[-5:]

@@ -137,9 +137,10 @@ def test_sharded_gpu_equals_single_process(tmp_path, n_subsets):
         single = rec.rho.astype(np.float64)
     r0, r1 = np.load(out.format(0)), np.load(out.format(1))
     assert np.array_equal(r0, r1)
-    # the shards' binary32 window sums round in another order than one
-    # process's, so the agreement is at the accumulation's own precision
-    assert np.linalg.norm(r0 - single) / np.linalg.norm(single) < 1e-5
+    # the shards' work items hold other events than one process's, so the
+    # per-item fixed-point roundings differ: agreement at the accumulation's
+    # own precision
+    assert np.linalg.norm(r0 - single) / np.linalg.norm(single) < 5e-5
     g = c1_geometry()
     ref = orc.mlem_f64(g, *ev, 3, n_subsets=n_subsets, sets_f32=True)
     assert np.linalg.norm(r0 - ref) / np.linalg.norm(ref) < 1e-4
@@ -164,4 +165,7 @@ def test_split_step_equals_iterate():
         b.update(1.0)
         assert float(acc.abs().sum()) == 0.0  # the update consumes the accumulator
         b.set_accumulator(None)
-        assert np.array_equal(a.rho, b.rho)
+        # the device-side binning places events in work items in an order
+        # that varies from run to run, and with it the per-item roundings
+        ra, rb = a.rho.astype(np.float64), b.rho.astype(np.float64)
+        assert np.linalg.norm(ra - rb) / np.linalg.norm(ra) < 2e-5
