@@ -47,8 +47,8 @@ PHANTOM = [
 SEED = 20260101
 # DRAM bytes (read + write) per event of one k_tile pass, from an ncu capture
 # of this workload's first 2e7 events (profiles/k_tile_strip_c2_2e7events.md:
-# 246.9 MB read + 7.9 MB written); the traffic grows with the event count.
-TILE_DRAM_BYTES_PER_EVENT = (246.890240e6 + 7.881472e6) / 2e7
+# 246.8 MB read + 5.0 MB written); the traffic grows with the event count.
+TILE_DRAM_BYTES_PER_EVENT = (246.809344e6 + 5.007360e6) / 2e7
 
 
 def workload_config(n_events, e2e_iters, world=1):
@@ -270,20 +270,18 @@ def ours(args, rank, world, local_rank):
     sc = scanner()
     n = args.events
 
-    # seeded workload in pinned host memory (rank r: seed + r)
+    # seeded workload (rank r: seed + r), generated on the GPU by the library's
+    # device generator (the host generator's events) and kept in pinned host
+    # memory for the end-to-end leg
+    import ctypes
     tz, zu = pinned_empty(n)
     td, zd = pinned_empty(n)
     tl, dl = pinned_empty(n)
-    from stripmlem import _lib
-    import ctypes
-    g = sc.geometry()
-    ph = (_lib.Ellipse * len(PHANTOM))(*[_lib.Ellipse(*map(float, e)) for e in PHANTOM])
-    rc = _lib.load().strip_generate_events(
-        ctypes.byref(g), ph, len(PHANTOM), SEED + rank, n,
-        zu.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
-        zd.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
-        dl.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
-    assert rc == 0, rc
+    gen = sm.generate_events_device(sc, PHANTOM, n, seed=SEED + rank, device=local_rank)
+    for host, dev in zip((tz, td, tl), gen):
+        host.copy_(dev)
+    del gen
+    torch.cuda.empty_cache()
 
     rec = sm.Reconstruction(sc, device=local_rank, mode=sm.MODE_CPU,
                             accumulation=sm.ACCUM_KAHAN)

@@ -298,6 +298,24 @@ int strip_generate_events_image(const strip_geometry* g, const float* rho,
                                 uint64_t seed, int64_t n, int uniform_angle,
                                 float* z_u, float* z_d, float* dl);
 
+/* The two generators on the current CUDA device, one thread per event, into
+ * DEVICE buffers d_z_u, d_z_d, d_dl of n floats each (rho stays a host
+ * image); return after the events are written.  Event i is the host
+ * generator's event i: the same Philox counters and the same binary64
+ * expressions, evaluated without FMA contraction on both sides, so results
+ * can differ only where the device math library rounds log, sin, cos or tan
+ * differently from the host's.  Replaces the reference's 2d_strip_phantom
+ * Monte Carlo loop (phantom_cmd.cpp:136-444, phantom_monte_carlo.h:29-109)
+ * for inputs of 1e8-1e9 events. */
+int strip_generate_events_device(const strip_geometry* g,
+                                 const strip_ellipse* ellipses, int n_ellipses,
+                                 uint64_t seed, int64_t n, float* d_z_u,
+                                 float* d_z_d, float* d_dl);
+int strip_generate_events_image_device(const strip_geometry* g,
+                                       const float* rho, uint64_t seed,
+                                       int64_t n, int uniform_angle,
+                                       float* d_z_u, float* d_z_d, float* d_dl);
+
 #ifdef __cplusplus
 }
 #endif

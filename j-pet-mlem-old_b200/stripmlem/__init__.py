@@ -326,6 +326,45 @@ def generate_events(scanner, ellipses, n, seed=1):
     return zu, zd, dl
 
 
+def generate_events_device(scanner, ellipses, n, seed=1, device=0):
+    """generate_events on the GPU (strip_generate_events_device): returns
+    three float32 CUDA tensors on ``device`` holding the same events."""
+    import torch
+    lib = _lib.load()
+    el = list(ellipses)
+    arr = (_lib.Ellipse * len(el))(*[_lib.Ellipse(*map(float, e)) for e in el])
+    out = [torch.empty(int(n), dtype=torch.float32, device=f"cuda:{device}")
+           for _ in range(3)]
+    g = scanner.geometry()
+    with torch.cuda.device(device):
+        torch.cuda.current_stream().synchronize()
+        rc = lib.strip_generate_events_device(ctypes.byref(g), arr, len(el), int(seed),
+                                              int(n), *(t.data_ptr() for t in out))
+    if rc != STRIP_OK:
+        raise StripError(rc, "strip_generate_events_device")
+    return tuple(out)
+
+
+def generate_events_image_device(scanner, rho, n, seed=1, uniform_angle=False, device=0):
+    """generate_events_image on the GPU (strip_generate_events_image_device)."""
+    import torch
+    lib = _lib.load()
+    img = np.ascontiguousarray(rho, dtype=np.float32)
+    if img.size != scanner.n_y_pixels * scanner.n_z_pixels:
+        raise ValueError("rho must hold n_y_pixels * n_z_pixels values")
+    out = [torch.empty(int(n), dtype=torch.float32, device=f"cuda:{device}")
+           for _ in range(3)]
+    g = scanner.geometry()
+    with torch.cuda.device(device):
+        torch.cuda.current_stream().synchronize()
+        rc = lib.strip_generate_events_image_device(
+            ctypes.byref(g), _fp(img), int(seed), int(n), int(bool(uniform_angle)),
+            *(t.data_ptr() for t in out))
+    if rc != STRIP_OK:
+        raise StripError(rc, "strip_generate_events_image_device")
+    return tuple(out)
+
+
 def generate_events_image(scanner, rho, n, seed=1, uniform_angle=False):
     """Seeded synthetic events emitted from an activity image
     (strip_generate_events_image); returns z_u, z_d, dl.  ``uniform_angle``

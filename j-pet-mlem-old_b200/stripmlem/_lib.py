@@ -150,6 +150,16 @@ SIGNATURES = {
         ctypes.c_int,
         [_P(Geometry), _P(Ellipse), ctypes.c_int, ctypes.c_uint64, ctypes.c_int64, _f, _f, _f],
     ),
+    "strip_generate_events_device": (
+        ctypes.c_int,
+        [_P(Geometry), _P(Ellipse), ctypes.c_int, ctypes.c_uint64, ctypes.c_int64,
+         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
+    "strip_generate_events_image_device": (
+        ctypes.c_int,
+        [_P(Geometry), _f, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int,
+         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
     "strip_generate_events_image": (
         ctypes.c_int,
         [_P(Geometry), _f, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int, _f, _f, _f],
