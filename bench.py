@@ -255,6 +255,87 @@ def differentiable_throughput(rec, n, reps=2):
     return tf / reps, ta / reps
 
 
+def batch_instances(n_inst=64):
+    """The batched workload: n_inst reconstructions, instance i seeded by i --
+    image n_y x n_z with n in [100, 800], pixel p in {1, 2, 3, 4} mm, strips
+    L = n_z p long at R = n_y p / 2, sigma_z 10 mm, sigma_dl 42 mm, 3-10
+    ellipses (the last a body covering most of the field), events
+    log-uniform in [1e5, 2e7]."""
+    out = []
+    for i in range(n_inst):
+        rng = np.random.default_rng(i)
+        n_y, n_z = (int(v) for v in rng.integers(100, 801, size=2))
+        p = float(rng.integers(1, 5))
+        R, L = n_y * p / 2.0, n_z * p
+        k = int(rng.integers(3, 11))
+        ph = []
+        for _ in range(k - 1):
+            ph.append((float(rng.uniform(-0.3, 0.3) * L), float(rng.uniform(-0.3, 0.3) * R),
+                       float(rng.uniform(0.04, 0.15) * L), float(rng.uniform(0.04, 0.15) * R),
+                       float(rng.uniform(0, 180)), float(rng.uniform(0.1, 2.0))))
+        ph.append((0.0, 0.0, 0.42 * L, 0.42 * R, 0.0, 1.0))
+        n_ev = int(np.exp(rng.uniform(np.log(1e5), np.log(2e7))))
+        out.append(dict(R=R, L=L, n_y=n_y, n_z=n_z, p=p, phantom=ph, events=n_ev, seed=i))
+    return out
+
+
+def batched_throughput(local_rank, n_inst, warmup, steps):
+    """The same instances advanced one context at a time (strip_iterate) and
+    as one batch (strip_batch_*): Mevent*iter/s of each over all events."""
+    import torch
+    import stripmlem as sm
+    recs = []
+    total = 0
+    try:
+        for inst in batch_instances(n_inst):
+            sc = sm.Scanner(inst["R"], inst["L"], inst["n_y"], inst["n_z"], inst["p"],
+                            inst["p"], 10.0, 42.0)
+            ev = sm.generate_events_device(sc, inst["phantom"], inst["events"],
+                                           seed=inst["seed"], device=local_rank)
+            rec = sm.Reconstruction(sc, device=local_rank, mode=sm.MODE_CPU)
+            rec.set_events_device(*ev)
+            del ev
+            recs.append(rec)
+            total += inst["events"]
+        torch.cuda.empty_cache()
+        import ctypes
+        flops = 0.0
+        overflow = 0
+        for rec in recs:
+            bb, inn, ne = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+            rec._check(rec.lib.strip_count_work(rec._ctx, ctypes.byref(bb), ctypes.byref(inn),
+                                                ctypes.byref(ne)))
+            flops += 10.0 * bb.value + 18.0 * inn.value
+            overflow += rec.stats()["n_overflow"]
+        seq_ms = 0.0
+        for rec in recs:
+            rec(None, warmup)
+            rec(None, steps)
+            seq_ms += rec.stats()["last_iterate_ms"]
+        with sm.Batch(recs) as batch:
+            batch(warmup)
+            batch(steps)
+            st = batch.stats()
+        bat_ms = st["last_iterate_ms"]
+        return {"instances": n_inst, "events": total, "steps": steps,
+                "sequential_Mevent_per_s": total * steps / (seq_ms / 1e3) / 1e6,
+                "batched_Mevent_per_s": total * steps / (bat_ms / 1e3) / 1e6,
+                "ratio_batched_vs_sequential": seq_ms / bat_ms,
+                "batched_ms_per_step": bat_ms / steps,
+                "work_model_tflops_batched": flops * steps / (bat_ms / 1e3) / 1e12,
+                "work_model_tflops_sequential": flops * steps / (seq_ms / 1e3) / 1e12,
+                "events_on_global_path": overflow,
+                "tile_work_items": st["n_work_items"],
+                "launches_per_step": st["launches_per_iteration"],
+                "what": "64 seeded instances (image 100-800 px per side, 1-4 mm pixels, "
+                        "1e5-2e7 events each): one MLEM step of every instance as one "
+                        "persistent tile launch + one update launch replayed from a CUDA "
+                        "graph, against strip_iterate on each context in turn"}
+    finally:
+        for r in recs:
+            r.close()
+
+
 def ours(args, rank, world, local_rank):
     import torch
     import stripmlem as sm
@@ -386,6 +467,13 @@ def ours(args, rank, world, local_rank):
                 "what": "strip_forward_device then strip_adjoint_device over the same "
                         "events (y_e = sum_j K_ej rho_j, g_j = sum_e K_ej / y_e)"}
 
+    batched = None
+    achieved_plain = flops_per_iter / (tile_ms / args.steps / 1e3) / 1e12
+    if world == 1 and not args.no_batched:
+        batched = batched_throughput(local_rank, 64, max(1, args.warmup // 3), 3)
+        batched["ratio_vs_plain_workload_by_work"] = (
+            batched["work_model_tflops_batched"] / achieved_plain)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = host_cores()
@@ -430,6 +518,8 @@ def ours(args, rank, world, local_rank):
         line["cpu_baseline"] = cpu
     if diff is not None:
         line["differentiable"] = diff
+    if batched is not None:
+        line["batched"] = batched
     if rank == 0:
         print(json.dumps(line), flush=True)
     if shd is not None:
@@ -452,6 +542,7 @@ def main():
     ap.add_argument("--ref-events", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-differentiable", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", 0))

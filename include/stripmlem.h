@@ -206,6 +206,51 @@ int strip_grad_sigma_device(strip_ctx* ctx, const float* d_rho,
                             const double* d_w, double sigma_z,
                             double sigma_dl, double* d_grad);
 
+/* ---- batches of reconstructions ----------------------------------------- */
+
+/* Several contexts -- each with its own geometry, events and image -- advanced
+ * together: one MLEM step is one persistent launch of the tile kernel over
+ * the work items of every member, the global-path launches of members with
+ * oversized event boxes, and one update launch over all images; the step is
+ * captured once as a CUDA graph and replayed.  The reference runs one
+ * reconstruction per process; there is no counterpart.
+ * Members (at most 64) share the device and the accumulation mode; their
+ * events are re-binned for plain MLEM (one subset).  A batch holds the
+ * members' buffers as they were at creation: re-create it after
+ * strip_set_events, strip_set_accumulator or a re-binning of a member
+ * (strip_set_image keeps the buffers).  While a batch iterates its members
+ * must not be used on other threads. */
+typedef struct strip_batch strip_batch;
+int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
+                       strip_batch** out);
+/* n_iter MLEM iterations of every member (no progress callbacks). */
+int strip_batch_iterate(strip_batch* b, int n_iter);
+/* Device time of the last strip_batch_iterate, the members' total events,
+ * the tile work items of one step and the kernel launches of one step. */
+int strip_batch_stats(strip_batch* b, double* last_iterate_ms,
+                      int64_t* n_events, int32_t* n_work_items,
+                      int32_t* launches_per_iteration);
+int strip_batch_last_error(strip_batch* b, char* buf, size_t size);
+int strip_batch_destroy(strip_batch* b);
+
+/* ---- schedule --------------------------------------------------------------- */
+
+/* A tile-kernel schedule: pixel tile edge, events a warp takes per counter
+ * step, and the measured device time of one backprojection with it. */
+typedef struct strip_tuning {
+  int32_t tile;
+  int32_t grab;
+  double ms;
+} strip_tuning;
+/* Times one MLEM backprojection of the context's events (into scratch: the
+ * image and accumulator are untouched) for every schedule of tile edge
+ * {16, 32, 48, 64} x grab {4, 8, 16}, keeps the fastest (events re-binned
+ * for it) and reports it in *best (may be NULL). */
+int strip_autotune(strip_ctx* ctx, int mode, strip_tuning* best);
+/* Sets the schedule by hand (tile edge 8..128, grab 1..32); re-bins the
+ * events when the context has some.  Defaults: tile 32, grab 8. */
+int strip_set_schedule(strip_ctx* ctx, int tile, int grab);
+
 /* ---- parity ----------------------------------------------------------- */
 
 /* For n host events (z_u, z_d, dl): bbox pixels tested, in-ellipse pixels and

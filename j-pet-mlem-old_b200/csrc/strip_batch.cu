@@ -1,0 +1,313 @@
+// Batched reconstructions and the schedule autotuner (include/stripmlem.h:
+// strip_batch_*, strip_autotune).
+//
+// A batch advances several contexts -- each with its own geometry, events and
+// image -- together: one MLEM step is ONE persistent launch of the tile kernel
+// over the work items of every member (k_tile_batch: CTAs pull items from a
+// global counter, largest first), the global-path launches of members that
+// have overflow events, and one update launch over all images; the step is
+// captured once as a CUDA graph and replayed.  The reference runs one
+// reconstruction per process (reconstruction_cmd.cpp:105-301); there is no
+// batched counterpart.
+//
+// The autotuner times one MLEM backprojection of a context's own events for
+// each candidate schedule -- pixel tile edge x events a warp takes per
+// counter step -- and keeps the fastest.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "strip_ctx.h"
+
+using namespace stripmlem;
+
+struct strip_batch {
+  int device = 0;
+  int mode = STRIP_MODE_CPU;
+  int accum = STRIP_ACCUM_KAHAN;
+  int sm_count = 148;
+  std::vector<strip_ctx*> members;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  BatchArgs* args = nullptr;  // host copy of the kernel parameters (~20 KB)
+  BatchItem* d_items = nullptr;
+  int n_items = 0;
+  int* d_counter = nullptr;
+  int smem_bytes = 0;
+  int64_t n_events = 0;
+  int launches_per_step = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  double last_ms = 0;
+  std::string err;
+};
+
+namespace {
+
+int bfail(strip_batch* b, int code, const std::string& msg) {
+  if (b) b->err = msg;
+  return code;
+}
+
+#define BCK(call)                                                             \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess)                                                    \
+      return bfail(b, e_ == cudaErrorMemoryAllocation ? STRIP_E_NOMEM         \
+                                                      : STRIP_E_CUDA,         \
+                   std::string(#call) + ": " + cudaGetErrorString(e_));       \
+  } while (0)
+
+void release(strip_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->d_items) cudaFree(b->d_items);
+  if (b->d_counter) cudaFree(b->d_counter);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b->args;
+  delete b;
+}
+
+// One step on the batch stream: counter reset, the persistent tile launch,
+// the members' global-path launches, the batched update.
+int enqueue_step(strip_batch* b) {
+  BCK(cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream));
+  BCK(launch_tile_batch(b->mode, b->accum, *b->args, b->d_items, b->n_items,
+                        b->d_counter, b->smem_bytes, b->sm_count, b->stream));
+  BatchUpdateArgs u{};
+  u.n = (int)b->members.size();
+  u.weighted = mlem_weighted(b->mode);
+  u.scale = 1.0;
+  int64_t max_pix = 0;
+  for (int m = 0; m < u.n; ++m) {
+    const LaunchArgs& a = b->args->member[m];
+    if (a.g_count > 0)
+      BCK(launch_global(OP_MLEM, b->mode, b->accum, a, b->stream));
+    u.rho[m] = b->members[m]->d_rho;
+    u.acc[m] = b->members[m]->d_acc;
+    u.n_pix[m] = b->members[m]->n_pix;
+    max_pix = std::max(max_pix, u.n_pix[m]);
+  }
+  BCK(launch_update_batch(u, max_pix, b->stream));
+  return STRIP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
+                       strip_batch** out) {
+  if (!members || !out || n_members <= 0 || n_members > kMaxBatch ||
+      (mode != STRIP_MODE_CPU && mode != STRIP_MODE_GPU))
+    return STRIP_E_INVALID;
+  *out = nullptr;
+  for (int m = 0; m < n_members; ++m) {
+    if (!members[m]) return STRIP_E_INVALID;
+    for (int k = 0; k < m; ++k)
+      if (members[k] == members[m]) return STRIP_E_INVALID;
+    if (members[m]->device != members[0]->device ||
+        members[m]->accum != members[0]->accum)
+      return ctx_fail(members[m], STRIP_E_INVALID,
+                      "strip_batch_create: members differ in device or accumulation");
+  }
+  strip_batch* b = new (std::nothrow) strip_batch();
+  if (!b) return STRIP_E_NOMEM;
+  b->args = new (std::nothrow) BatchArgs();
+  if (!b->args) {
+    delete b;
+    return STRIP_E_NOMEM;
+  }
+  b->device = members[0]->device;
+  b->mode = mode;
+  b->accum = members[0]->accum;
+  b->sm_count = members[0]->sm_count;
+  b->members.assign(members, members + n_members);
+  int rc = STRIP_OK;
+  std::vector<BatchItem> items;
+  for (int m = 0; m < n_members && rc == STRIP_OK; ++m) {
+    strip_ctx* c = members[m];
+    rc = ctx_prepare_mlem(c, mode);
+    if (rc != STRIP_OK) {
+      b->err = "member " + std::to_string(m) + ": " + c->err;
+      break;
+    }
+    b->args->member[m] = ctx_mlem_args(c, mode);
+    b->smem_bytes = std::max(b->smem_bytes, c->t.smem_bytes);
+    b->n_events += c->n_events;
+    for (int i = 0; i < b->args->member[m].n_items; ++i) {
+      const WorkItem& w = c->items[i];
+      items.push_back(BatchItem{m, w.tile, w.count, 0, w.begin});
+    }
+    b->launches_per_step += b->args->member[m].g_count > 0;
+  }
+  if (rc == STRIP_OK) {
+    // largest items first: the persistent CTAs then finish close together
+    std::stable_sort(items.begin(), items.end(),
+                     [](const BatchItem& x, const BatchItem& y) { return x.count > y.count; });
+    b->n_items = (int)items.size();
+    b->launches_per_step += 2;  // tile + update
+    do {
+      if (cudaSetDevice(b->device) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
+      if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
+        rc = STRIP_E_CUDA;
+        break;
+      }
+      if (cudaMalloc(&b->d_items, std::max<size_t>(items.size(), 1) * sizeof(BatchItem)) != cudaSuccess ||
+          cudaMalloc(&b->d_counter, sizeof(int)) != cudaSuccess) {
+        rc = STRIP_E_NOMEM;
+        break;
+      }
+      if (!items.empty() &&
+          cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(BatchItem),
+                     cudaMemcpyHostToDevice) != cudaSuccess) {
+        rc = STRIP_E_CUDA;
+        break;
+      }
+      // the members' own streams may still hold work on their buffers
+      for (strip_ctx* c : b->members)
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc = STRIP_E_CUDA;
+      if (rc != STRIP_OK) break;
+      // capture one step as a graph (kernel attributes are set beforehand)
+      if (tile_batch_reserve_smem(b->mode, b->accum, b->smem_bytes) != cudaSuccess ||
+          cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        rc = STRIP_E_CUDA;
+        break;
+      }
+      const int erc = enqueue_step(b);
+      const cudaError_t ec = cudaStreamEndCapture(b->stream, &b->graph);
+      if (erc != STRIP_OK) { rc = erc; break; }
+      if (ec != cudaSuccess ||
+          cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess) {
+        rc = STRIP_E_CUDA;
+        break;
+      }
+    } while (0);
+    if (rc != STRIP_OK && b->err.empty()) b->err = cudaGetErrorString(cudaGetLastError());
+  }
+  if (rc != STRIP_OK) {
+    cudaGetLastError();
+    for (strip_ctx* c : b->members)
+      if (c->err.empty()) c->err = "strip_batch_create: " + b->err;
+    release(b);
+    return rc;
+  }
+  *out = b;
+  return STRIP_OK;
+}
+
+int strip_batch_iterate(strip_batch* b, int n_iter) {
+  if (!b || n_iter < 0) return STRIP_E_INVALID;
+  BCK(cudaSetDevice(b->device));
+  BCK(cudaEventRecord(b->ev0, b->stream));
+  for (int it = 0; it < n_iter; ++it) BCK(cudaGraphLaunch(b->exec, b->stream));
+  BCK(cudaEventRecord(b->ev1, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+  b->last_ms = ms;
+  return STRIP_OK;
+}
+
+int strip_batch_stats(strip_batch* b, double* last_iterate_ms, int64_t* n_events,
+                      int32_t* n_work_items, int32_t* launches_per_iteration) {
+  if (!b) return STRIP_E_INVALID;
+  if (last_iterate_ms) *last_iterate_ms = b->last_ms;
+  if (n_events) *n_events = b->n_events;
+  if (n_work_items) *n_work_items = b->n_items;
+  if (launches_per_iteration) *launches_per_iteration = b->launches_per_step;
+  return STRIP_OK;
+}
+
+int strip_batch_last_error(strip_batch* b, char* buf, size_t size) {
+  if (!b || !buf || size == 0) return STRIP_E_INVALID;
+  std::snprintf(buf, size, "%s", b->err.c_str());
+  return STRIP_OK;
+}
+
+int strip_batch_destroy(strip_batch* b) {
+  if (!b) return STRIP_E_INVALID;
+  release(b);
+  return STRIP_OK;
+}
+
+int strip_autotune(strip_ctx* ctx, int mode, strip_tuning* best) {
+  if (!ctx || (mode != STRIP_MODE_CPU && mode != STRIP_MODE_GPU))
+    return STRIP_E_INVALID;
+  if (int rc = ctx_prepare_mlem(ctx, mode)) return rc;
+  static const int kTiles[] = {16, 32, 48, 64};
+  static const int kGrabs[] = {4, 8, 16};
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    return ctx_fail(ctx, STRIP_E_CUDA, "strip_autotune: cudaEventCreate failed");
+  }
+  double* d_scratch = nullptr;  // the backprojections go here, not into acc
+  if (cudaMalloc(&d_scratch, ctx->n_pix * sizeof(double)) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return ctx_fail(ctx, STRIP_E_NOMEM, "strip_autotune: no memory for the scratch image");
+  }
+  strip_tuning top{0, 0, 0.0};
+  int rc = STRIP_OK;
+  for (int tile : kTiles) {
+    if ((rc = ctx_rebin(ctx, tile)) != STRIP_OK) break;
+    if (mode == STRIP_MODE_GPU && (rc = ctx_prepare_mlem(ctx, mode)) != STRIP_OK) break;
+    for (int grab : kGrabs) {
+      ctx->grab = grab;
+      LaunchArgs a = ctx_mlem_args(ctx, mode);
+      a.acc = d_scratch;
+      float best_ms = 1e30f;
+      for (int rep = 0; rep < 3 && rc == STRIP_OK; ++rep) {  // the first is a warm-up
+        cudaError_t e = cudaEventRecord(e0, ctx->stream);
+        if (e == cudaSuccess) e = launch_tile(OP_MLEM, mode, ctx->accum, a, ctx->stream);
+        if (e == cudaSuccess) e = launch_global(OP_MLEM, mode, ctx->accum, a, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess) {
+          rc = ctx_fail(ctx, STRIP_E_CUDA, cudaGetErrorString(e));
+          break;
+        }
+        if (rep > 0) best_ms = std::min(best_ms, ms);
+      }
+      if (rc != STRIP_OK) break;
+      if (top.tile == 0 || best_ms < top.ms) top = strip_tuning{tile, grab, best_ms};
+    }
+    if (rc != STRIP_OK) break;
+  }
+  cudaFree(d_scratch);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != STRIP_OK) return rc;
+  ctx->grab = top.grab;
+  if (int r2 = ctx_rebin(ctx, top.tile)) return r2;
+  if (best) *best = top;
+  return STRIP_OK;
+}
+
+int strip_set_schedule(strip_ctx* ctx, int tile, int grab) {
+  if (!ctx) return STRIP_E_INVALID;
+  if (tile < 8 || tile > 128 || grab < 1 || grab > 32)
+    return ctx_fail(ctx, STRIP_E_INVALID, "strip_set_schedule: tile in [8, 128], grab in [1, 32]");
+  ctx->grab = grab;
+  if (ctx->n_subsets <= 0) {  // no events yet: used by the next binning
+    ctx->tile_pref = tile;
+    return STRIP_OK;
+  }
+  return ctx_rebin(ctx, tile);
+}
+
+}  // extern "C"

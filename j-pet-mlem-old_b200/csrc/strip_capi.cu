@@ -17,44 +17,9 @@
 
 #include "stripmlem.h"
 #include "strip_internal.h"
+#include "strip_ctx.h"
 
 using namespace stripmlem;
-
-struct strip_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  char devname[256] = {0};
-  int sm_count = 148;
-  int smem_optin = 227 * 1024;
-  strip_geometry g{};
-  ScannerF s{};
-  int accum = STRIP_ACCUM_KAHAN;
-  int64_t n_pix = 0;
-  float* d_rho = nullptr;
-  double* d_acc = nullptr;      // accumulator in use (own or the caller's)
-  double* d_acc_own = nullptr;  // the context's own accumulator
-  int acc_mode = STRIP_MODE_CPU;  // mode of the last strip_accumulate
-  float* d_sens5 = nullptr;
-  // binned events
-  int64_t n_events = 0;   // as given by the caller
-  int64_t n_binned = 0;   // events with a non-empty box
-  float* d_zu = nullptr;
-  float* d_zd = nullptr;
-  float* d_dl = nullptr;
-  int64_t* d_perm = nullptr;
-  int n_subsets = 0;
-  Tiling t{};
-  int max_w = 0, max_h = 0;
-  std::vector<WorkItem> items;
-  WorkItem* d_items = nullptr;
-  std::vector<int> sub_item_begin, sub_item_count;
-  std::vector<int64_t> sub_g_begin, sub_g_count;
-  int* d_status = nullptr;
-  std::vector<cudaEvent_t> tile_marks;
-  strip_stats stats{};
-  std::string err;
-};
 
 namespace {
 
@@ -154,10 +119,8 @@ Tiling choose_tiling(const strip_ctx* ctx, int max_w, int max_h) {
   const int n_z = ctx->s.n_z, n_y = ctx->s.n_y;
   const int budget = std::min(ctx->smem_optin, 113 * 1024);
   Tiling t{};
-  int TX = 32, TY = 32;
+  int TX = ctx->tile_pref, TY = ctx->tile_pref;
   int HX = max_w / 2 + 2, HY = max_h / 2 + 2;
-  // per-warp event tables hold a whole event box when it has <= 128 rows
-  t.row_cap = std::min(128, std::max(32, (max_h + 31) / 32 * 32));
   for (;;) {
     const int WX = std::min(n_z, TX + 2 * HX), WY = std::min(n_y, TY + 2 * HY);
     // Row stride = 2 (mod 32): the 32 lanes of a warp walk runs on 32
@@ -166,9 +129,7 @@ Tiling choose_tiling(const strip_ctx* ctx, int max_w, int max_h) {
     // ellipses over the banks best (fewest shared-memory wavefronts in a
     // simulation over events of the 800 x 400 geometry).
     const int WS = WX + ((2 - WX % 32) + 32) % 32;
-    // groups of a block of row_cap rows whose runs fit a window row
-    t.bit_words = (t.row_cap * ((WX + 2) / 3) + 31) / 32 + 1;
-    const int bytes = tile_smem_bytes(WY, WS, t.row_cap, t.bit_words);
+    const int bytes = tile_smem_bytes(WY, WS);
     if (bytes <= budget || (HX <= 8 && HY <= 8)) {
       t.TX = TX;
       t.TY = TY;
@@ -343,6 +304,7 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
   ctx->sub_g_begin.swap(gb);
   ctx->sub_g_count.swap(gc);
   ctx->n_binned = (int64_t)total;
+  dfree(ctx->d_wbin);  // sized for the previous binning
   ctx->n_subsets = n_subsets;
   ctx->t = t;
   ctx->max_w = wh[0];
@@ -396,9 +358,7 @@ LaunchArgs base_args(strip_ctx* ctx) {
   a.rho = ctx->d_rho;
   a.acc = ctx->d_acc;
   a.status = ctx->d_status;
-  // global path: blocks of 32 rows of at most max_w columns
-  a.gcap = 32;
-  a.gbit_words = (32 * ((std::max(ctx->max_w, 1) + 2) / 3) + 31) / 32 + 1;
+  a.grab = ctx->grab;
   return a;
 }
 
@@ -500,6 +460,7 @@ int strip_ctx_destroy(strip_ctx* ctx) {
   dfree(ctx->d_rho);
   dfree(ctx->d_acc_own);
   dfree(ctx->d_sens5);
+  dfree(ctx->d_wbin);
   dfree(ctx->d_zu);
   dfree(ctx->d_zd);
   dfree(ctx->d_dl);
@@ -787,10 +748,19 @@ int adjoint_dev(strip_ctx* ctx, const double* d_w, double sz, double sdl,
   if (mode == STRIP_MODE_GPU)
     if (int rc = ensure_sens5(ctx)) return rc;
   CK(cudaMemsetAsync(d_g, 0, ctx->n_pix * sizeof(double), ctx->stream));
+  // the weights in binned order (read contiguously by the kernels)
+  if (!ctx->d_wbin && ctx->n_binned > 0)
+    CK(cudaMalloc(&ctx->d_wbin, ctx->n_binned * sizeof(double)));
+  CK(launch_gather_weights(ctx->d_perm, d_w, ctx->n_binned, ctx->d_wbin,
+                           ctx->stream));
   LaunchArgs a = base_args(ctx);
   a.k = make_kernel(sz, sdl, ctx->s.pw);
   a.acc = d_g;
-  a.w_in = d_w;
+  a.w_in = ctx->d_wbin;
+  // GaussianKernel values are at most kc / sqrt(2 R^2 ipsz): E <= 1 and
+  // a'Sa >= ipsz (ap^2 + aq^2) >= 2 R^2 ipsz sec^4
+  a.kbound = (float)((double)a.k.kc /
+                     ((double)ctx->s.R * std::sqrt(2.0 * (double)a.k.ipsz)) * 1.02);
   if (int rc = run_all(ctx, OP_ADJOINT, mode, a)) return rc;
   if (mode == STRIP_MODE_GPU)
     CK(launch_scale_copy(d_g, ctx->d_sens5, d_g, ctx->n_pix, ctx->stream));
@@ -1018,3 +988,42 @@ int strip_debug_pixel_sets(strip_ctx* ctx, const float* zu, const float* zd,
 }
 
 }  // extern "C"
+
+// ---- internal entry points for strip_batch.cu (strip_ctx.h) -------------
+namespace stripmlem {
+
+int ctx_fail(strip_ctx* ctx, int code, const char* msg) {
+  return fail(ctx, code, "%s", msg);
+}
+
+int ctx_prepare_mlem(strip_ctx* ctx, int mode) {
+  if (int rc = check_ready(ctx)) return rc;
+  if (int rc = set_device(ctx)) return rc;
+  if (int rc = ensure_binning(ctx, 1)) return rc;
+  if (mode == STRIP_MODE_GPU)
+    if (int rc = ensure_sens5(ctx)) return rc;
+  return STRIP_OK;
+}
+
+LaunchArgs ctx_mlem_args(strip_ctx* ctx, int mode) {
+  LaunchArgs a = base_args(ctx);
+  a.sens = (mode == STRIP_MODE_GPU) ? ctx->d_sens5 : nullptr;
+  a.items = ctx->d_items;
+  a.n_items = ctx->sub_item_count.empty() ? 0 : ctx->sub_item_count[0];
+  a.g_begin = ctx->sub_g_begin.empty() ? 0 : ctx->sub_g_begin[0];
+  a.g_count = ctx->sub_g_count.empty() ? 0 : ctx->sub_g_count[0];
+  return a;
+}
+
+int ctx_rebin(strip_ctx* ctx, int tile) {
+  if (int rc = check_ready(ctx)) return rc;
+  if (int rc = set_device(ctx)) return rc;
+  ctx->tile_pref = tile;
+  const int n_subsets = ctx->n_subsets;
+  ctx->n_subsets = -1;  // force a new binning at the same subset count
+  const int rc = ensure_binning(ctx, n_subsets);
+  if (rc != STRIP_OK) ctx->n_subsets = n_subsets;
+  return rc;
+}
+
+}  // namespace stripmlem

@@ -1,0 +1,64 @@
+// The strip context (opaque in include/stripmlem.h) and the internal entry
+// points strip_batch.cu uses.  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "stripmlem.h"
+#include "strip_internal.h"
+
+struct strip_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  char devname[256] = {0};
+  int sm_count = 148;
+  int smem_optin = 227 * 1024;
+  strip_geometry g{};
+  stripmlem::ScannerF s{};
+  int accum = STRIP_ACCUM_KAHAN;
+  int64_t n_pix = 0;
+  float* d_rho = nullptr;
+  double* d_acc = nullptr;      // accumulator in use (own or the caller's)
+  double* d_acc_own = nullptr;  // the context's own accumulator
+  int acc_mode = STRIP_MODE_CPU;  // mode of the last strip_accumulate
+  int tile_pref = 32;  // tile edge in pixels (autotuned or 32)
+  int grab = 8;        // events a warp takes per counter step (autotuned or 8)
+  float* d_sens5 = nullptr;
+  double* d_wbin = nullptr;     // adjoint weights in binned order (n_binned)
+  // binned events
+  int64_t n_events = 0;   // as given by the caller
+  int64_t n_binned = 0;   // events with a non-empty box
+  float* d_zu = nullptr;
+  float* d_zd = nullptr;
+  float* d_dl = nullptr;
+  int64_t* d_perm = nullptr;
+  int n_subsets = 0;
+  stripmlem::Tiling t{};
+  int max_w = 0, max_h = 0;
+  std::vector<stripmlem::WorkItem> items;
+  stripmlem::WorkItem* d_items = nullptr;
+  std::vector<int> sub_item_begin, sub_item_count;
+  std::vector<int64_t> sub_g_begin, sub_g_count;
+  int* d_status = nullptr;
+  std::vector<cudaEvent_t> tile_marks;
+  strip_stats stats{};
+  std::string err;
+};
+
+namespace stripmlem {
+
+// Records msg as the context's last error and returns code.
+int ctx_fail(strip_ctx* ctx, int code, const char* msg);
+// Device selected, events binned for plain MLEM (one subset), the 5-point
+// sensitivity present for STRIP_MODE_GPU.
+int ctx_prepare_mlem(strip_ctx* ctx, int mode);
+// Launch arguments of one MLEM step of the (single) subset.
+LaunchArgs ctx_mlem_args(strip_ctx* ctx, int mode);
+// Re-bins the events with `tile` x `tile` pixel tiles.
+int ctx_rebin(strip_ctx* ctx, int tile);
+
+}  // namespace stripmlem

@@ -47,9 +47,7 @@ __host__ __device__ inline int fixed_shift(int count) {
 struct Tiling {
   int TX, TY, HX, HY, ntx, nty, n_tiles;
   int WXmax, WYmax, WS;
-  int row_cap;     // rows per per-warp event table (multiple of 32)
-  int bit_words;   // words of the per-warp row-start bitmap
-  int smem_bytes;  // windows + per-warp event tables
+  int smem_bytes;  // the two shared-memory windows
 };
 
 __host__ __device__ inline void tile_window(const Tiling& t, int n_z, int n_y,
@@ -90,11 +88,36 @@ struct LaunchArgs {
   int64_t g_begin;       // global-path event range [g_begin, g_begin+g_count)
   int64_t g_count;
   double* y_out;         // OP_FORWARD: per event (caller order)
-  const double* w_in;    // OP_ADJOINT / OP_GRAD: per event weights (caller order)
+  const double* w_in;    // OP_ADJOINT: per event weights in binned order;
+                         // OP_GRAD: in the caller's order
   double* grad_out;      // OP_GRAD: 2 doubles (atomic)
   double sz, sdl;        // OP_GRAD: model sigmas
-  int gcap, gbit_words;  // event tables of the global path
+  float kbound;          // OP_ADJOINT: bound of the GaussianKernel values
+  int grab;              // events a warp takes per counter step (1..32)
   int* status;           // device status word (0 = ok)
+};
+
+// Several reconstructions in one persistent launch (strip_batch.cu): the
+// members' arguments travel in the kernel parameter space (up to 32 KB).
+constexpr int kMaxBatch = 64;
+struct BatchArgs {
+  LaunchArgs member[kMaxBatch];
+};
+static_assert(sizeof(BatchArgs) <= 32000, "batch arguments exceed the parameter space");
+struct BatchItem {
+  int32_t member;
+  int32_t tile;
+  int32_t count;
+  int32_t pad;
+  int64_t begin;
+};
+struct BatchUpdateArgs {
+  int n;
+  int weighted;
+  double scale;
+  float* rho[kMaxBatch];
+  double* acc[kMaxBatch];
+  int64_t n_pix[kMaxBatch];
 };
 
 // ---- host helpers (strip_capi.cu) ------------------------------------------
@@ -104,8 +127,7 @@ ScannerF make_scanner(const strip_geometry& g);
 KernelF make_kernel(double sigma_z, double sigma_dl, float pw);
 
 // ---- launchers (strip_kernels.cu) ----------------------------------------
-int tile_smem_bytes(int WYmax, int WS, int row_cap, int bit_words);
-int global_smem_bytes(int cap, int bit_words);
+int tile_smem_bytes(int WYmax, int WS);
 cudaError_t launch_event_boxes(const ScannerF& s, const float* zu,
                                const float* zd, const float* dl, int64_t n,
                                int4* boxes, int* max_wh, unsigned long long* n_empty,
@@ -134,6 +156,17 @@ cudaError_t launch_update_out(const float* rho_in, float* rho_out,
                               cudaStream_t st);
 // Whether MLEM in `mode` accumulates rho-weighted contributions.
 inline int mlem_weighted(int mode) { return mode == STRIP_MODE_CPU; }
+// out_i = w[perm_i]: caller-order weights into binned order
+cudaError_t launch_gather_weights(const int64_t* perm, const double* w,
+                                  int64_t n, double* out, cudaStream_t st);
+// Sets the batched tile kernel's dynamic shared-memory limit (before a
+// launch is captured into a graph).
+cudaError_t tile_batch_reserve_smem(int mode, int accum, int smem_bytes);
+cudaError_t launch_tile_batch(int mode, int accum, const BatchArgs& b,
+                              const BatchItem* items, int n_items, int* counter,
+                              int smem_bytes, int sm_count, cudaStream_t st);
+cudaError_t launch_update_batch(const BatchUpdateArgs& u, int64_t max_pix,
+                                cudaStream_t st);
 cudaError_t launch_sensitivity(const ScannerF& s, int five_point, float* out,
                                cudaStream_t st);
 cudaError_t launch_debug_sets(const ScannerF& s, const float* zu,

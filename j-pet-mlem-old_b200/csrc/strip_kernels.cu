@@ -23,6 +23,8 @@
 // Reference behaviour: Reconstruction::bb_update (src/2d/strip/reconstruction.h:
 // 220-298) and the warp kernel (src/2d/strip/cuda/reconstruction/
 // warp_granularity.cuh:20-176).
+#include <algorithm>
+
 #include "strip_internal.h"
 #include "strip_rows.cuh"
 
@@ -32,7 +34,6 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kThreads = 512;
-constexpr int kGrab = 8;  // events a warp takes from the item per counter step
 constexpr int kWarps = kThreads / 32;
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -86,49 +87,74 @@ struct RowSum<STRIP_ACCUM_FP64> {
   __device__ __forceinline__ double total() const { return s; }
 };
 
-// Binary32 -> unsigned integer by the 2^23 addend: for 0 <= x * s < 2^23 the
+// Binary32 -> integer by a power-of-two addend: for 0 <= x * s < 2^23 the
 // bits of x * s + 2^23 (one FFMA, round to nearest) minus those of 2^23 are
-// round(x * s).
+// round(x * s); for |x * s| < 2^22 the same with 1.5 * 2^23 gives the
+// two's-complement round(x * s).
 constexpr float kMagic = 8388608.0f;
 constexpr unsigned kMagicBits = 0x4B000000u;
+constexpr float kMagicSigned = 12582912.0f;
+constexpr unsigned kMagicSignedBits = 0x4B400000u;
 __device__ __forceinline__ unsigned to_fixed(float x, float s) {
   return __float_as_uint(fmaf(x, s, kMagic)) - kMagicBits;
 }
 
-// Shared-memory window of the image: w = rho (* s), acc = partial
-// backprojection -- binary32 (acc) or, for the rho-weighted MLEM
-// accumulation, 2^kFixedShift fixed point (acc_u).
-// FINE: scales above 2^22 (items of fewer than ~1000 events) convert with
-// cvt.rni (the conversion pipe) instead of the 2^23 addend.
-template <bool FINE>
+// How a shared-memory window accumulates the backprojection:
+//   kAccF32     binary32 atomics (a load and a compare-and-swap per add here)
+//   kAccU32     unsigned fixed point, the 2^23 addend (rho-weighted MLEM)
+//   kAccU32Cvt  unsigned fixed point, cvt.rni (scales above 2^22)
+//   kAccS32     signed fixed point, the 1.5 * 2^23 addend (adjoint)
+// The fixed-point kinds use native 32-bit integer shared atomics; the scale
+// `fixed_unit` is a power of two chosen per work item so that no sum wraps.
+enum AccKind { kAccF32 = 0, kAccU32 = 1, kAccU32Cvt = 2, kAccS32 = 3 };
+
+template <int KIND>
 struct SmemWin {
   const float* w;
   float* acc;
   int wx0, wy0, WS;
-  float fixed_unit;  // 2^fixed_shift(item events)
-  __device__ __forceinline__ float unit() const { return fixed_unit; }
+  float fixed_unit;
+  __device__ __forceinline__ float unit() const {
+    return KIND == kAccF32 ? 1.0f : fixed_unit;
+  }
   __device__ __forceinline__ int ptr(int iy, int col) const {
     return (iy - wy0) * WS + (col - wx0);
   }
   __device__ __forceinline__ float read(int p, int j) const { return w[p + j]; }
+  // acc_j += v (v already scaled by unit())
   __device__ __forceinline__ void add(int p, int j, float v) const {
-    atomicAdd(acc + p + j, v);
+    if constexpr (KIND == kAccS32)
+      atomicAdd(reinterpret_cast<int*>(acc) + p + j,
+                (int)(__float_as_uint(v + kMagicSigned) - kMagicSignedBits));
+    else
+      atomicAdd(acc + p + j, v);
   }
   // acc_j += K_j w_j / D_e for K_j = E * pref and sc = pref / D_e * unit()
   __device__ __forceinline__ void add_weighted(int p, int j, float E,
                                                float sc) const {
-    const unsigned v = FINE ? __float2uint_rn(E * w[p + j] * sc)
-                            : to_fixed(E * w[p + j], sc);
+    const unsigned v = KIND == kAccU32Cvt ? __float2uint_rn(E * w[p + j] * sc)
+                                          : to_fixed(E * w[p + j], sc);
     atomicAdd(reinterpret_cast<unsigned*>(acc) + p + j, v);
   }
+  // acc_j += P.x * sc, acc_j+1 += P.y * sc (signed fixed point)
+  __host__ __device__ static constexpr bool pair_add() { return KIND == kAccS32; }
+  __device__ __forceinline__ void add2(int p, int j, f32x2 P, float sc) const {
+    const float2 x = unpack2(fma2(P, pack2(sc, sc),
+                                  pack2(kMagicSigned, kMagicSigned)));
+    int* ai = reinterpret_cast<int*>(acc) + p + j;
+    atomicAdd(ai, (int)(__float_as_uint(x.x) - kMagicSignedBits));
+    atomicAdd(ai + 1, (int)(__float_as_uint(x.y) - kMagicSignedBits));
+  }
   // the same for pixels j, j + 1 with K = P * pref (packed)
-  static constexpr bool kPairScatter = true;
+  __host__ __device__ static constexpr bool pair_scatter() {
+    return KIND == kAccU32 || KIND == kAccU32Cvt;
+  }
   __device__ __forceinline__ void add_weighted2(int p, int j, f32x2 P,
                                                 float sc) const {
     unsigned* au = reinterpret_cast<unsigned*>(acc) + p + j;
     const f32x2 kw = mul2(P, pack2(w[p + j], w[p + j + 1]));
     unsigned v0, v1;
-    if constexpr (FINE) {
+    if constexpr (KIND == kAccU32Cvt) {
       const float2 x = unpack2(mul2(kw, pack2(sc, sc)));
       v0 = __float2uint_rn(x.x);
       v1 = __float2uint_rn(x.y);
@@ -162,7 +188,9 @@ struct GlobalWin {
     atomicAdd(acc + p + j, (double)v);
   }
   __device__ __forceinline__ float unit() const { return 1.0f; }
-  static constexpr bool kPairScatter = false;
+  __host__ __device__ static constexpr bool pair_scatter() { return false; }
+  __host__ __device__ static constexpr bool pair_add() { return false; }
+  __device__ __forceinline__ void add2(int64_t, int, f32x2, float) const {}
   __device__ __forceinline__ void add_weighted(int64_t p, int j, float E,
                                                float sc) const {
     atomicAdd(acc + p + j, (double)(E * read(p, j) * sc));
@@ -341,7 +369,7 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
       const auto p = win.ptr(e.tly + ranked_row(H, rank0 + 32 * b + lane),
                              run_lo(L.lolen[b]));
       if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED && kPairs &&
-                    Win::kPairScatter) {
+                    Win::pair_scatter()) {
         PairRecurrence g(k, L.E0[b], L.R0[b]);
         const float sc = fminf(L.pref[b] * scale * win.unit(), 3.0e38f);
 #pragma unroll 2
@@ -359,9 +387,18 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
           E *= R;
           R *= k.q;
         }
+      } else if constexpr (MODE == STRIP_MODE_CPU && kPairs && Win::pair_add()) {
+        PairRecurrence g(k, L.E0[b], L.R0[b]);
+        const float sc = L.pref[b] * scale * win.unit();
+#pragma unroll 2
+        for (int j = 0; j + 1 < n; j += 2) {
+          win.add2(p, j, g.P, sc);
+          g.step();
+        }
+        if (n & 1) win.add(p, n - 1, unpack2(g.P).x * sc);
       } else if constexpr (MODE == STRIP_MODE_CPU) {
         float E = L.E0[b], R = L.R0[b];
-        const float sc = L.pref[b] * scale;
+        const float sc = L.pref[b] * scale * win.unit();
 #pragma unroll 4
         for (int j = 0; j < n; ++j) {
           win.add(p, j, E * sc);
@@ -459,7 +496,7 @@ __device__ __forceinline__ void process_event(const LaunchArgs& a,
     if (!(D > 0.0)) return;
     scale = (float)(1.0 / D);
   } else {
-    scale = (float)a.w_in[a.perm[pos]];
+    scale = (float)a.w_in[pos];  // OP_ADJOINT: weights in binned order
     if (scale == 0.0f) return;
   }
   constexpr bool kWeighted = OP == OP_MLEM && MODE == STRIP_MODE_CPU;
@@ -479,25 +516,56 @@ __device__ __forceinline__ RowTables warp_tables(char* base, int cap, int warp) 
   return row_tables_at(base + (size_t)warp * row_table_bytes(cap), cap);
 }
 
-// The events of a work item: warps pull groups of kGrab events from a shared
-// counter until the item is done (lanes < kGrab set the group's events up in
-// parallel).
+// Fixed-point scale of an adjoint work item: every addend is K_j w_e with
+// K_j <= a.kbound (the GaussianKernel's bound, E <= 1 and a'Sa >= 2 R^2 ipsz)
+// and |w_e| <= W, the item's largest weight, so with B = kbound * W the
+// scale 2^s keeps each addend below 2^22 and the item's sum below 2^31.
+__device__ int adjoint_shift(const LaunchArgs& a, const WorkItem& it, int lane) {
+  __shared__ float s_wmax[kWarps];
+  __shared__ int s_shift;
+  float m = 0.0f;
+  for (int64_t i = it.begin + threadIdx.x; i < it.begin + it.count;
+       i += blockDim.x)
+    m = fmaxf(m, fabsf((float)a.w_in[i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(kFull, m, o));
+  if (lane == 0) s_wmax[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float W = 0.0f;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) W = fmaxf(W, s_wmax[i]);
+    const float B = a.kbound * W * 1.0001f;
+    const float n = (float)it.count + (float)(it.count >> 7) + 1.0f;
+    const float lim = fminf(4194304.0f, 2147483648.0f / n);
+    int sh = 0;
+    if (B > 0.0f && B < 3.0e38f)
+      sh = (int)floorf(log2f(lim / B)) - 1;
+    s_shift = max(-120, min(120, sh));
+  }
+  __syncthreads();
+  return s_shift;
+}
+
+// The events of a work item: warps pull groups of a.grab (1..32) events from
+// a shared counter until the item is done (lanes < a.grab set the group's
+// events up in parallel).
 template <int OP, int MODE, int ACC, class Win>
 __device__ __forceinline__ void run_item(const LaunchArgs& a, const WorkItem& it,
                                          const Win& win, int lane,
                                          int* next_group) {
   const int64_t end = it.begin + it.count;
+  const int grab = a.grab;
   for (;;) {
     int g = 0;
     if (lane == 0) g = atomicAdd(next_group, 1);
     g = __shfl_sync(kFull, g, 0);
-    const int64_t base = it.begin + (int64_t)g * kGrab;
+    const int64_t base = it.begin + (int64_t)g * grab;
     if (base >= end) break;
     const int64_t ei = base + lane;
     EventF mine = {};
-    if (lane < kGrab && ei < end)
+    if (lane < grab && ei < end)
       event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], mine);
-    const int nh = (int)min((int64_t)kGrab, end - base);
+    const int nh = (int)min((int64_t)grab, end - base);
     for (int j = 0; j < nh; ++j) {
       const EventF e = shfl_event(mine, j);
       process_event<OP, MODE, ACC>(a, e, win, lane, base + j);
@@ -505,17 +573,19 @@ __device__ __forceinline__ void run_item(const LaunchArgs& a, const WorkItem& it
   }
 }
 
+// One work item on the whole CTA: stage the window, run the events, flush.
+// The CTA may run further items afterwards (the batched kernel): the caller
+// synchronises before the shared memory is reused.
 template <int OP, int MODE, int ACC>
-__global__ void __launch_bounds__(kThreads, 2) k_tile(LaunchArgs a) {  // 2 CTAs x 16 warps per SM
-  extern __shared__ __align__(16) char smem_raw[];
-  const WorkItem it = a.items[blockIdx.x];
+__device__ __forceinline__ void tile_item(const LaunchArgs& a,
+                                          const WorkItem it, char* smem_raw,
+                                          int* s_next_group) {
   int wx0, wy0, wx1, wy1;
   tile_window(a.t, a.s.n_z, a.s.n_y, it.tile, wx0, wy0, wx1, wy1);
   const int wxn = wx1 - wx0, wyn = wy1 - wy0, WS = a.t.WS;
   float* s_w = reinterpret_cast<float*>(smem_raw);
   float* s_acc = s_w + a.t.WYmax * WS;
-  __shared__ int s_next_group;
-  if (threadIdx.x == 0) s_next_group = 0;
+  if (threadIdx.x == 0) *s_next_group = 0;
   const int lane = threadIdx.x & 31;
   constexpr bool kReads = (OP != OP_ADJOINT);
   constexpr bool kWrites = (OP == OP_MLEM || OP == OP_ADJOINT);
@@ -530,28 +600,95 @@ __global__ void __launch_bounds__(kThreads, 2) k_tile(LaunchArgs a) {  // 2 CTAs
     if (kWrites) s_acc[r * WS + c] = 0.0f;
   }
   __syncthreads();
-  const int fshift = fixed_shift(it.count);
-  const float unit = (float)(1u << fshift);
-  if (fshift > 22)
-    run_item<OP, MODE, ACC>(a, it, SmemWin<true>{s_w, s_acc, wx0, wy0, WS, unit},
-                            lane, &s_next_group);
-  else
-    run_item<OP, MODE, ACC>(a, it, SmemWin<false>{s_w, s_acc, wx0, wy0, WS, unit},
-                            lane, &s_next_group);
+  // fixed-point scale 2^fshift of the window accumulator
+  int fshift = 0;
+  if constexpr (OP == OP_MLEM && MODE == STRIP_MODE_CPU) {
+    fshift = fixed_shift(it.count);
+  } else if constexpr (OP == OP_ADJOINT && MODE == STRIP_MODE_CPU) {
+    fshift = adjoint_shift(a, it, lane);
+  }
+  const float unit = exp2f((float)fshift);
+  if constexpr (OP == OP_MLEM && MODE == STRIP_MODE_CPU) {
+    if (fshift > 22)
+      run_item<OP, MODE, ACC>(
+          a, it, SmemWin<kAccU32Cvt>{s_w, s_acc, wx0, wy0, WS, unit}, lane,
+          s_next_group);
+    else
+      run_item<OP, MODE, ACC>(
+          a, it, SmemWin<kAccU32>{s_w, s_acc, wx0, wy0, WS, unit}, lane,
+          s_next_group);
+  } else if constexpr (OP == OP_ADJOINT && MODE == STRIP_MODE_CPU) {
+    run_item<OP, MODE, ACC>(a, it,
+                            SmemWin<kAccS32>{s_w, s_acc, wx0, wy0, WS, unit},
+                            lane, s_next_group);
+  } else {
+    run_item<OP, MODE, ACC>(a, it,
+                            SmemWin<kAccF32>{s_w, s_acc, wx0, wy0, WS, 1.0f},
+                            lane, s_next_group);
+  }
   if (kWrites) {
     __syncthreads();
-    constexpr bool kFixed = OP == OP_MLEM && MODE == STRIP_MODE_CPU;
     const unsigned* s_acc_u = reinterpret_cast<const unsigned*>(s_acc);
+    const int* s_acc_i = reinterpret_cast<const int*>(s_acc);
     for (int q = threadIdx.x; q < wxn * wyn; q += blockDim.x) {
       const int r = q / wxn, c = q - r * wxn;
       double v;
-      if constexpr (kFixed)
+      if constexpr (OP == OP_MLEM && MODE == STRIP_MODE_CPU)
         v = ldexp((double)s_acc_u[r * WS + c], -fshift);
+      else if constexpr (OP == OP_ADJOINT && MODE == STRIP_MODE_CPU)
+        v = ldexp((double)s_acc_i[r * WS + c], -fshift);
       else
         v = (double)s_acc[r * WS + c];
       if (v != 0.0)
         atomicAdd(a.acc + (int64_t)(wy0 + r) * a.s.n_z + wx0 + c, v);
     }
+  }
+}
+
+template <int OP, int MODE, int ACC>
+__global__ void __launch_bounds__(kThreads, 2) k_tile(LaunchArgs a) {  // 2 CTAs x 16 warps per SM
+  extern __shared__ __align__(16) char smem_raw[];
+  __shared__ int s_next_group;
+  tile_item<OP, MODE, ACC>(a, a.items[blockIdx.x], smem_raw, &s_next_group);
+}
+
+// Persistent tile kernel over the work items of several reconstructions: a
+// CTA takes item after item from a global counter; item i belongs to member
+// items[i].member, whose arguments live in the kernel's parameter space.
+template <int MODE, int ACC>
+__global__ void __launch_bounds__(kThreads, 2)
+    k_tile_batch(const __grid_constant__ BatchArgs b, const BatchItem* items,
+                 int n_items, int* counter) {
+  extern __shared__ __align__(16) char smem_raw[];
+  __shared__ int s_next_group;
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int i = s_item;
+    if (i >= n_items) break;
+    const BatchItem bi = items[i];
+    tile_item<OP_MLEM, MODE, ACC>(b.member[bi.member],
+                                  WorkItem{bi.tile, bi.count, bi.begin},
+                                  smem_raw, &s_next_group);
+    __syncthreads();  // before the next item's window overwrites this one
+  }
+}
+
+// rho_j <- acc_j * scale (or rho_j * acc_j * scale), acc_j <- 0 for every
+// member: blockIdx.y selects the member.
+__global__ void k_update_batch(const __grid_constant__ BatchUpdateArgs u) {
+  const int m = blockIdx.y;
+  if (m >= u.n) return;
+  float* rho = u.rho[m];
+  double* acc = u.acc[m];
+  const int64_t n = u.n_pix[m];
+  const int weighted = u.weighted;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    rho[j] = weighted ? (float)(acc[j] * u.scale)
+                      : (float)((double)rho[j] * acc[j] * u.scale);
+    acc[j] = 0.0;
   }
 }
 
@@ -660,6 +797,13 @@ __global__ void k_bin_scatter(const int* keys, int64_t n, const float* zu,
       operm[p] = orig ? orig[i] : i;
     }
   }
+}
+
+__global__ void k_gather_weights(const int64_t* perm, const double* w,
+                                 int64_t n, double* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = w[perm[i]];
 }
 
 __global__ void k_update_out(const float* rho_in, float* rho_out,
@@ -839,17 +983,8 @@ cudaError_t launch_global_t(const LaunchArgs& a, cudaStream_t st) {
     return FN<op, STRIP_MODE_GPU, STRIP_ACCUM_KAHAN>(a, st);               \
   } while (0)
 
-int tile_smem_bytes(int WYmax, int WS, int row_cap, int bit_words) {
-  (void)row_cap;
-  (void)bit_words;
-  return 2 * WYmax * WS * 4;
-}
-
-int global_smem_bytes(int cap, int bit_words) {
-  (void)cap;
-  (void)bit_words;
-  return 0;
-}
+// Two windows (the image and the accumulator) of WYmax rows of stride WS.
+int tile_smem_bytes(int WYmax, int WS) { return 2 * WYmax * WS * 4; }
 
 cudaError_t launch_tile(int op, int mode, int accum, const LaunchArgs& a,
                         cudaStream_t st) {
@@ -887,6 +1022,46 @@ cudaError_t launch_global(int op, int mode, int accum, const LaunchArgs& a,
   }
 }
 
+template <class F>
+cudaError_t with_tile_batch(int mode, int accum, F&& pick) {
+  if (mode == STRIP_MODE_CPU) {
+    if (accum == STRIP_ACCUM_FP32) return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP32>);
+    if (accum == STRIP_ACCUM_FP64) return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP64>);
+    return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_KAHAN>);
+  }
+  if (accum == STRIP_ACCUM_FP32) return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_FP32>);
+  if (accum == STRIP_ACCUM_FP64) return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_FP64>);
+  return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_KAHAN>);
+}
+
+cudaError_t tile_batch_reserve_smem(int mode, int accum, int smem_bytes) {
+  return with_tile_batch(mode, accum, [&](auto fn) {
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem_bytes);
+  });
+}
+
+cudaError_t launch_tile_batch(int mode, int accum, const BatchArgs& b,
+                              const BatchItem* items, int n_items, int* counter,
+                              int smem_bytes, int sm_count, cudaStream_t st) {
+  if (n_items <= 0) return cudaSuccess;
+  auto pick = [&](auto fn) -> cudaError_t {
+    const int grid = std::min(n_items, sm_count * 2);
+    fn<<<grid, kThreads, smem_bytes, st>>>(b, items, n_items, counter);
+    return cudaGetLastError();
+  };
+  return with_tile_batch(mode, accum, pick);
+}
+
+
+cudaError_t launch_update_batch(const BatchUpdateArgs& u, int64_t max_pix,
+                                cudaStream_t st) {
+  if (u.n <= 0) return cudaSuccess;
+  const int gx = (int)std::min<int64_t>(std::max<int64_t>((max_pix + kThreads - 1) / kThreads, 1), 64);
+  k_update_batch<<<dim3(gx, u.n), kThreads, 0, st>>>(u);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_event_boxes(const ScannerF& s, const float* zu,
                                const float* zd, const float* dl, int64_t n,
                                int4* boxes, int* max_wh,
@@ -922,6 +1097,13 @@ cudaError_t launch_update(float* rho, double* acc, int64_t n_pix, double scale,
                           int weighted, cudaStream_t st) {
   k_update<<<grid_for(n_pix), kThreads, 0, st>>>(rho, acc, n_pix, scale,
                                                  weighted);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_weights(const int64_t* perm, const double* w,
+                                  int64_t n, double* out, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  k_gather_weights<<<grid_for(n), kThreads, 0, st>>>(perm, w, n, out);
   return cudaGetLastError();
 }
 

@@ -230,6 +230,19 @@ class Reconstruction:
 
     iterate = __call__
 
+    # -- schedule -----------------------------------------------------------
+    def autotune(self, mode=None):
+        """Times the tile-kernel schedules on this context's events and keeps
+        the fastest (strip_autotune); returns {'tile', 'grab', 'ms'}."""
+        t = _lib.Tuning()
+        self._check(self.lib.strip_autotune(self._ctx, self.mode if mode is None else mode,
+                                            ctypes.byref(t)))
+        self.n_subsets = 1
+        return {"tile": t.tile, "grab": t.grab, "ms": t.ms}
+
+    def set_schedule(self, tile=32, grab=8):
+        self._check(self.lib.strip_set_schedule(self._ctx, int(tile), int(grab)))
+
     # -- split iteration (events sharded over processes) -------------------
     def set_accumulator(self, acc):
         """Makes ``acc`` (a float64 CUDA tensor of n_y * n_z values on this
@@ -304,6 +317,69 @@ class Reconstruction:
             nin.ctypes.data_as(P(ctypes.c_int32)),
             dig.ctypes.data_as(P(ctypes.c_uint64))))
         return nbb, nin, dig
+
+
+class Batch:
+    """Several Reconstructions (each with its own geometry, events and
+    image) advanced together: one persistent tile launch and one update
+    launch per MLEM step, replayed from a CUDA graph (strip_batch_*).
+    Re-create the batch after set_events on a member."""
+
+    def __init__(self, reconstructions, mode=MODE_CPU):
+        self.lib = _lib.load()
+        self.members = list(reconstructions)
+        arr = (ctypes.c_void_p * len(self.members))(*[r._ctx.value for r in self.members])
+        h = ctypes.c_void_p()
+        rc = self.lib.strip_batch_create(arr, len(self.members), int(mode), ctypes.byref(h))
+        if rc != STRIP_OK:
+            msgs = []
+            for r in self.members:
+                buf = ctypes.create_string_buffer(512)
+                self.lib.strip_last_error(r._ctx, buf, 512)
+                if buf.value:
+                    msgs.append(buf.value.decode(errors="replace"))
+            raise StripError(rc, "; ".join(msgs) or "strip_batch_create")
+        self._h = h
+        for r in self.members:
+            r.n_subsets = 1
+
+    def _check(self, rc):
+        if rc != STRIP_OK:
+            buf = ctypes.create_string_buffer(512)
+            self.lib.strip_batch_last_error(self._h, buf, 512)
+            raise StripError(rc, buf.value.decode(errors="replace"))
+
+    def __call__(self, n_iterations=1):
+        self._check(self.lib.strip_batch_iterate(self._h, int(n_iterations)))
+
+    iterate = __call__
+
+    def stats(self):
+        ms = ctypes.c_double()
+        ne = ctypes.c_int64()
+        items = ctypes.c_int32()
+        launches = ctypes.c_int32()
+        self._check(self.lib.strip_batch_stats(self._h, ctypes.byref(ms), ctypes.byref(ne),
+                                               ctypes.byref(items), ctypes.byref(launches)))
+        return {"last_iterate_ms": ms.value, "n_events": ne.value,
+                "n_work_items": items.value, "launches_per_iteration": launches.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.strip_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def generate_events(scanner, ellipses, n, seed=1):

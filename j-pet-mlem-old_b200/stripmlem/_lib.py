@@ -48,6 +48,10 @@ class Geometry(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("tile", ctypes.c_int32), ("grab", ctypes.c_int32), ("ms", ctypes.c_double)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("n_events", ctypes.c_int64),
@@ -132,6 +136,16 @@ SIGNATURES = {
         [_ctx, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
          ctypes.c_void_p],
     ),
+    "strip_batch_create": (
+        ctypes.c_int, [_P(ctypes.c_void_p), ctypes.c_int, ctypes.c_int, _P(ctypes.c_void_p)]),
+    "strip_batch_iterate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "strip_batch_stats": (
+        ctypes.c_int,
+        [ctypes.c_void_p, _d, _P(ctypes.c_int64), _P(ctypes.c_int32), _P(ctypes.c_int32)]),
+    "strip_batch_last_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
+    "strip_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "strip_autotune": (ctypes.c_int, [_ctx, ctypes.c_int, _P(Tuning)]),
+    "strip_set_schedule": (ctypes.c_int, [_ctx, ctypes.c_int, ctypes.c_int]),
     "strip_debug_pixel_sets": (
         ctypes.c_int,
         [_ctx, _f, _f, _f, ctypes.c_int64, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_uint64)],
