@@ -26,6 +26,9 @@
 
 using namespace stripmlem;
 
+// Windows up to this size let two CTAs share an SM.
+constexpr int kNarrowSmem = 113 * 1024;
+
 struct strip_batch {
   int device = 0;
   int mode = STRIP_MODE_CPU;
@@ -35,10 +38,14 @@ struct strip_batch {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   BatchArgs* args = nullptr;  // host copy of the kernel parameters (~20 KB)
+  // Work items in two shared-memory classes: members whose windows fit two
+  // CTAs per SM, and wide-window members (one CTA per SM).  Each class is one
+  // persistent launch, so a wide member does not halve the occupancy of the
+  // others.  Class c owns items [cls_begin[c], cls_begin[c] + cls_count[c]).
   BatchItem* d_items = nullptr;
   int n_items = 0;
-  int* d_counter = nullptr;
-  int smem_bytes = 0;
+  int cls_begin[2] = {0, 0}, cls_count[2] = {0, 0}, cls_smem[2] = {0, 0};
+  int* d_counter = nullptr;  // one counter per class
   int64_t n_events = 0;
   int launches_per_step = 0;
   cudaGraph_t graph = nullptr;
@@ -81,9 +88,13 @@ void release(strip_batch* b) {
 // One step on the batch stream: counter reset, the persistent tile launch,
 // the members' global-path launches, the batched update.
 int enqueue_step(strip_batch* b) {
-  BCK(cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream));
-  BCK(launch_tile_batch(b->mode, b->accum, *b->args, b->d_items, b->n_items,
-                        b->d_counter, b->smem_bytes, b->sm_count, b->stream));
+  BCK(cudaMemsetAsync(b->d_counter, 0, 2 * sizeof(int), b->stream));
+  for (int c = 0; c < 2; ++c)
+    if (b->cls_count[c] > 0)
+      BCK(launch_tile_batch(b->mode, b->accum, *b->args,
+                            b->d_items + b->cls_begin[c], b->cls_count[c],
+                            b->d_counter + c, b->cls_smem[c], b->sm_count,
+                            b->stream));
   BatchUpdateArgs u{};
   u.n = (int)b->members.size();
   u.weighted = mlem_weighted(b->mode);
@@ -143,20 +154,26 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
       break;
     }
     b->args->member[m] = ctx_mlem_args(c, mode);
-    b->smem_bytes = std::max(b->smem_bytes, c->t.smem_bytes);
+    const int cls = c->t.smem_bytes > kNarrowSmem;
+    b->cls_smem[cls] = std::max(b->cls_smem[cls], c->t.smem_bytes);
     b->n_events += c->n_events;
     for (int i = 0; i < b->args->member[m].n_items; ++i) {
       const WorkItem& w = c->items[i];
-      items.push_back(BatchItem{m, w.tile, w.count, 0, w.begin});
+      items.push_back(BatchItem{m, w.tile, w.count, cls, w.begin});
     }
     b->launches_per_step += b->args->member[m].g_count > 0;
   }
   if (rc == STRIP_OK) {
-    // largest items first: the persistent CTAs then finish close together
+    // by class, then largest items first: the persistent CTAs of a class
+    // then finish close together
     std::stable_sort(items.begin(), items.end(),
-                     [](const BatchItem& x, const BatchItem& y) { return x.count > y.count; });
+                     [](const BatchItem& x, const BatchItem& y) {
+                       return x.pad != y.pad ? x.pad < y.pad : x.count > y.count;
+                     });
     b->n_items = (int)items.size();
-    b->launches_per_step += 2;  // tile + update
+    for (const BatchItem& it : items) ++b->cls_count[it.pad];
+    b->cls_begin[1] = b->cls_count[0];
+    b->launches_per_step += 1 + (b->cls_count[0] > 0) + (b->cls_count[1] > 0);
     do {
       if (cudaSetDevice(b->device) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
       if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -165,7 +182,7 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
         break;
       }
       if (cudaMalloc(&b->d_items, std::max<size_t>(items.size(), 1) * sizeof(BatchItem)) != cudaSuccess ||
-          cudaMalloc(&b->d_counter, sizeof(int)) != cudaSuccess) {
+          cudaMalloc(&b->d_counter, 2 * sizeof(int)) != cudaSuccess) {
         rc = STRIP_E_NOMEM;
         break;
       }
@@ -180,7 +197,8 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
         if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc = STRIP_E_CUDA;
       if (rc != STRIP_OK) break;
       // capture one step as a graph (kernel attributes are set beforehand)
-      if (tile_batch_reserve_smem(b->mode, b->accum, b->smem_bytes) != cudaSuccess ||
+      if (tile_batch_reserve_smem(b->mode, b->accum,
+                                  std::max(b->cls_smem[0], b->cls_smem[1])) != cudaSuccess ||
           cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         rc = STRIP_E_CUDA;
         break;

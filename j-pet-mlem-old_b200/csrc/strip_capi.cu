@@ -114,10 +114,14 @@ int set_device(strip_ctx* ctx) {
 }
 
 // Chooses the tile size and halos for the largest event box, within the
-// shared memory available to 2 CTAs per SM.
+// shared memory of 2 CTAs per SM; when even 16 x 16 tiles leave the halos too
+// large for that, within the shared memory of one CTA per SM (half the
+// resident warps, but every event stays on the shared-memory path) before
+// the halos shrink and the largest boxes fall to the global-memory path.
 Tiling choose_tiling(const strip_ctx* ctx, int max_w, int max_h) {
   const int n_z = ctx->s.n_z, n_y = ctx->s.n_y;
-  const int budget = std::min(ctx->smem_optin, 113 * 1024);
+  const int wide_budget = ctx->smem_optin - 2048;  // static shared memory
+  int budget = std::min(ctx->smem_optin, 113 * 1024);
   Tiling t{};
   int TX = ctx->tile_pref, TY = ctx->tile_pref;
   int HX = max_w / 2 + 2, HY = max_h / 2 + 2;
@@ -143,6 +147,11 @@ Tiling choose_tiling(const strip_ctx* ctx, int max_w, int max_h) {
     }
     if (TX > 16 || TY > 16) {
       TX = TY = 16;
+      continue;
+    }
+    if (budget < wide_budget) {
+      budget = wide_budget;
+      TX = TY = ctx->tile_pref;
       continue;
     }
     if (HX >= HY) HX = HX * 3 / 4; else HY = HY * 3 / 4;

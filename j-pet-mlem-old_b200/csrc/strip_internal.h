@@ -108,7 +108,7 @@ struct BatchItem {
   int32_t member;
   int32_t tile;
   int32_t count;
-  int32_t pad;
+  int32_t pad;    // host-side: the item's shared-memory class
   int64_t begin;
 };
 struct BatchUpdateArgs {
