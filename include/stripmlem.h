@@ -248,7 +248,7 @@ typedef struct strip_tuning {
  * for it) and reports it in *best (may be NULL). */
 int strip_autotune(strip_ctx* ctx, int mode, strip_tuning* best);
 /* Sets the schedule by hand (tile edge 8..128, grab 1..32); re-bins the
- * events when the context has some.  Defaults: tile 32, grab 8. */
+ * events when the context has some.  Defaults: tile 32, grab 16. */
 int strip_set_schedule(strip_ctx* ctx, int tile, int grab);
 
 /* ---- parity ----------------------------------------------------------- */

@@ -26,7 +26,7 @@ struct strip_ctx {
   double* d_acc_own = nullptr;  // the context's own accumulator
   int acc_mode = STRIP_MODE_CPU;  // mode of the last strip_accumulate
   int tile_pref = 32;  // tile edge in pixels (autotuned or 32)
-  int grab = 8;        // events a warp takes per counter step (autotuned or 8)
+  int grab = 16;       // events a warp takes per counter step (autotuned or 16)
   float* d_sens5 = nullptr;
   double* d_wbin = nullptr;     // adjoint weights in binned order (n_binned)
   // binned events
