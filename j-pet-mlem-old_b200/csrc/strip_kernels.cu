@@ -425,13 +425,39 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
 // the same recurrence as pass 1 while s0 = sum E w and s2 = sum E w t^2 are
 // gathered, so the row's share is pref * (fz s0 + 2 ipsz s2) / sz and
 // pref * fdl * s0 / sdl.
+// Per-event data besides the event itself, loaded by the lane that sets the
+// event up (so the dependent global loads overlap instead of stalling the
+// warp at every event): OP_FORWARD the caller's index of the event,
+// OP_ADJOINT its weight (binned order), OP_GRAD its weight (caller order).
+struct EventAux {
+  int64_t out = 0;
+  double w = 0.0;
+};
+
+template <int OP>
+__device__ __forceinline__ EventAux load_aux(const LaunchArgs& a, int64_t pos) {
+  EventAux x;
+  if constexpr (OP == OP_FORWARD) x.out = a.perm[pos];
+  if constexpr (OP == OP_ADJOINT) x.w = a.w_in[pos];
+  if constexpr (OP == OP_GRAD) x.w = a.w_in[a.perm[pos]];
+  return x;
+}
+
+template <int OP>
+__device__ __forceinline__ EventAux shfl_aux(const EventAux& m, int src) {
+  EventAux x;
+  if constexpr (OP == OP_FORWARD) x.out = __shfl_sync(kFull, m.out, src);
+  if constexpr (OP == OP_ADJOINT || OP == OP_GRAD)
+    x.w = __shfl_sync(kFull, m.w, src);
+  return x;
+}
+
 template <class Win>
 __device__ __forceinline__ void grad_event(const LaunchArgs& a,
                                            const EventF& e,
                                            const EventRows& er, int H,
                                            const Win& win, int lane,
-                                           int64_t pos) {
-  const double w = a.w_in[a.perm[pos]];
+                                           double w) {
   if (w == 0.0) return;
   double gz = 0.0, gdl = 0.0;
   for (int i = lane; i < H; i += 32) {
@@ -469,12 +495,12 @@ __device__ __forceinline__ void grad_event(const LaunchArgs& a,
 template <int OP, int MODE, int ACC, class Win>
 __device__ __forceinline__ void process_event(const LaunchArgs& a,
                                               const EventF& e, const Win& win,
-                                              int lane, int64_t pos) {
+                                              int lane, const EventAux& aux) {
   const int H = e.bry - e.tly;
   if (H <= 0 || e.brx <= e.tlx) return;
   const EventRows er = event_rows(a.s, e);
   if constexpr (OP == OP_GRAD) {
-    grad_event(a, e, er, H, win, lane, pos);
+    grad_event(a, e, er, H, win, lane, aux.w);
     return;
   }
   constexpr int kSuper = 32 * kRowBlocks;
@@ -489,14 +515,14 @@ __device__ __forceinline__ void process_event(const LaunchArgs& a,
     }
     const double D = warp_sum(acc.total());
     if (OP == OP_FORWARD) {
-      if (lane == 0) a.y_out[a.perm[pos]] = D;
+      if (lane == 0) a.y_out[aux.out] = D;
       return;
     }
     // reconstruction.h:290 -- an all-zero denominator contributes nothing
     if (!(D > 0.0)) return;
     scale = (float)(1.0 / D);
   } else {
-    scale = (float)a.w_in[pos];  // OP_ADJOINT: weights in binned order
+    scale = (float)aux.w;  // OP_ADJOINT
     if (scale == 0.0f) return;
   }
   constexpr bool kWeighted = OP == OP_MLEM && MODE == STRIP_MODE_CPU;
@@ -563,12 +589,15 @@ __device__ __forceinline__ void run_item(const LaunchArgs& a, const WorkItem& it
     if (base >= end) break;
     const int64_t ei = base + lane;
     EventF mine = {};
-    if (lane < grab && ei < end)
+    EventAux aux;
+    if (lane < grab && ei < end) {
+      aux = load_aux<OP>(a, ei);
       event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], mine);
+    }
     const int nh = (int)min((int64_t)grab, end - base);
     for (int j = 0; j < nh; ++j) {
       const EventF e = shfl_event(mine, j);
-      process_event<OP, MODE, ACC>(a, e, win, lane, base + j);
+      process_event<OP, MODE, ACC>(a, e, win, lane, shfl_aux<OP>(aux, j));
     }
   }
 }
@@ -702,11 +731,15 @@ __global__ void __launch_bounds__(kThreads) k_global(LaunchArgs a) {
   for (int64_t base = a.g_begin + wid * 32; base < end; base += nwt * 32) {
     const int64_t ei = base + lane;
     EventF mine = {};
-    if (ei < end) event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], mine);
+    EventAux aux;
+    if (ei < end) {
+      aux = load_aux<OP>(a, ei);
+      event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], mine);
+    }
     const int nh = (int)min((int64_t)32, end - base);
     for (int j = 0; j < nh; ++j) {
       const EventF e = shfl_event(mine, j);
-      process_event<OP, MODE, ACC>(a, e, win, lane, base + j);
+      process_event<OP, MODE, ACC>(a, e, win, lane, shfl_aux<OP>(aux, j));
     }
   }
 }
