@@ -318,6 +318,21 @@ typedef struct strip_ellipse {
   double z, y, a, b, angle_deg, activity;
 } strip_ellipse;
 
+/* A phantom region of the reference's phantom description
+ * (phantom.h:137-181; z is the file's x): ellipse (centre, axes a, b,
+ * rotation in degrees), rectangle (centre, half sides a, b) or point
+ * (centre); intensity per unit area (per point). */
+enum strip_region_kind {
+  STRIP_REGION_ELLIPSE = 0,
+  STRIP_REGION_RECTANGLE = 1,
+  STRIP_REGION_POINT = 2
+};
+typedef struct strip_region {
+  int32_t kind;
+  int32_t reserved;
+  double z, y, a, b, angle_deg, intensity;
+} strip_region;
+
 /* Seeded host generator of list-mode events in the reference's event format.
  * Emission points are uniform in the union of the ellipses, overlaps
  * exclusive with the first-listed ellipse on top (phantom.h:193-204);
@@ -360,6 +375,49 @@ int strip_generate_events_image_device(const strip_geometry* g,
                                        const float* rho, uint64_t seed,
                                        int64_t n, int uniform_angle,
                                        float* d_z_u, float* d_z_d, float* d_dl);
+
+/* The reference's phantom Monte Carlo (2d_strip_phantom: phantom_cmd.cpp:
+ * 136-444, phantom_monte_carlo.h:29-109, phantom.h:120-215) on the current
+ * CUDA device, one thread per emission index:
+ *   additive       overlapping regions add up instead of the first-listed
+ *                  region covering the later ones (--additive)
+ *   uniform_angle  emission angle uniform in (-pi/2, pi/2), the tool's
+ *                  model; 0: tan(theta) uniform over the acceptance
+ *   count_emitted  n counts emissions and only the detected ones are
+ *                  written, in emission order (the tool without --detected);
+ *                  0: n detected events (--detected)
+ *   d_emitted, d_detected  optional DEVICE images of n_z x n_y counts
+ *                  (uint32) of the emission points of all / the detected
+ *                  emissions, on the tool's pixel grid of pixel_size centred
+ *                  at (origin_z, origin_y): column = floor((z - z0) / s),
+ *                  row = floor((y - y0) / s), row 0 at the bottom; counts
+ *                  are added to what the images hold.
+ * Events go to DEVICE buffers of n floats each; *n_written receives their
+ * number and *n_emitted the number of emissions (either may be NULL).
+ * Random streams: Philox-4x32-10 counters (seed, index), not the reference's
+ * tausworthe generator, so the events are the reference's in distribution,
+ * not in value. */
+typedef struct strip_simulation {
+  int32_t additive;
+  int32_t uniform_angle;
+  int32_t count_emitted;
+  int32_t reserved;
+  uint32_t* d_emitted;
+  uint32_t* d_detected;
+  double pixel_size, origin_z, origin_y;
+} strip_simulation;
+int strip_simulate_device(const strip_geometry* g, const strip_region* regions,
+                          int n_regions, const strip_simulation* options,
+                          uint64_t seed, int64_t n, float* d_z_u, float* d_z_d,
+                          float* d_dl, int64_t* n_written, int64_t* n_emitted);
+/* The same with HOST buffers on CUDA device `device`: z_u, z_d, dl hold n
+ * floats each (the first *n_written are set); emitted / detected are
+ * n_y x n_z hit images (may be NULL; the d_ fields of options are ignored). */
+int strip_simulate(const strip_geometry* g, const strip_region* regions,
+                   int n_regions, const strip_simulation* options,
+                   uint64_t seed, int64_t n, int device, float* z_u,
+                   float* z_d, float* dl, uint32_t* emitted, uint32_t* detected,
+                   int64_t* n_written, int64_t* n_emitted);
 
 #ifdef __cplusplus
 }

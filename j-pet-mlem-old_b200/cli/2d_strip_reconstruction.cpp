@@ -26,208 +26,37 @@
 
 #include "stripmlem.h"
 #include "strip_io.h"
+#include "strip_options.h"
 
 namespace {
 
-// ---------------------------------------------------------------------------
-// options: the reference's option set (options.cpp:13-76, reconstruction_cmd
-// .cpp:114-115, common/options.cpp:5-20) and its parser semantics
-// (lib/cmdline: --name=value, --name value, -x value, -abc flags; config
-// files hold one argument per line, '#' lines ignored; options marked
-// not_from_file ignore config files).
-// ---------------------------------------------------------------------------
-struct Option {
-  std::string name;
-  char short_name;
-  bool has_value;
-  bool not_from_file;
-  std::string def;
-  std::string help;
-  std::string value;
-  int count = 0;
-};
+using strip_cli::Options;
+using strip_cli::add_index;
+using strip_cli::ext_of;
+using strip_cli::wo_ext;
+using strip_cli::wo_path;
 
-class Options {
- public:
-  Options() {
-    add("config", 'c', true, false, "", "load config file");
-    add("radius", 'r', true, false, "0.5", "R distance between scintillator");
-    add("length", 'l', true, false, "1", "scintillator length");
-    add("s-pixel", 'p', true, false, "0.01", "pixel size");
-    add("n-pixels", 'n', true, false, "0", "number of pixels");
-    add("n-z-pixels", 0, true, false, "", "number of z pixels");
-    add("n-y-pixels", 0, true, false, "", "number of y pixels");
-    add("s-z", 0, true, false, "0.015", "TOF sigma along z axis");
-    add("s-dl", 0, true, false, "0.06", "TOF sigma delta-l");
-    add("n-emissions", 'e', true, true, "0", "number of emissions");
-    add("verbose", 'v', false, false, "", "print progress information (-v) or benchmark (-vv)");
-    add("n-threads", 'T', true, false, "", "number of host threads");
-    add("3d-response", 0, false, false, "", "input response contains additional LOR information");
-    add("dl-is-time", 0, false, false, "", "delta is time, convert using speed of light");
-    add("speed-of-light", 0, true, false, "299792458", "speed of light");
-    add("scale-length", 0, true, false, "1", "scale input length values");
-    add("scale-time", 0, true, false, "1", "scale input time values");
-    add("blocks", 'i', true, false, "0", "number of iteration blocks");
-    add("iterations", 'I', true, false, "1", "number of iterations (per block)");
-    add("output", 'o', true, true, "", "output files prefix (png)");
-    add("png-max", 0, true, false, "0", "maximum value mapped to 255 in PNG");
-    add("gpu", 'G', false, false, "", "use the reference's GPU semantics");
-    add("cuda-device", 'D', true, false, "0", "CUDA device");
-    add("cuda-blocks", 'B', true, false, "64", "CUDA blocks (accepted, unused)");
-    add("cuda-threads", 'W', true, false, "512", "CUDA threads per block (accepted, unused)");
-    add("rho", 0, true, false, "", "start rho (eg. existing iteration)");
-    add("rho-is-int", 0, false, false, "", "start rho uses integer representation (not float)");
-    add("help", 'h', false, false, "", "print this message");
-    add("dump-responses", 0, true, true, "",
-        "write the responses as read (after unit conversion) to this binary file and exit");
-  }
-
-  void parse(const std::vector<std::string>& args, bool from_file) {
-    for (size_t i = 0; i < args.size(); ++i) {
-      const std::string& a = args[i];
-      if (a.compare(0, 2, "--") == 0) {
-        const auto eq = a.find('=');
-        const std::string name = a.substr(2, eq == std::string::npos ? std::string::npos : eq - 2);
-        Option& o = get(name);
-        if (eq != std::string::npos) {
-          set(o, a.substr(eq + 1), from_file);
-        } else if (o.has_value) {
-          if (i + 1 >= args.size()) throw "option needs value: --" + name;
-          set(o, args[++i], from_file);
-        } else {
-          set(o, "", from_file);
-        }
-      } else if (a.size() > 1 && a[0] == '-') {
-        for (size_t j = 1; j < a.size(); ++j) {
-          Option& o = get_short(a[j]);
-          const bool last = j + 1 == a.size();
-          if (last && o.has_value && i + 1 < args.size()) {
-            set(o, args[++i], from_file);
-          } else if (o.has_value) {
-            throw std::string("option needs value: -") + a[j];
-          } else {
-            set(o, "", from_file);
-          }
-        }
-      } else if (a != "-") {
-        rest.push_back(a);
-      }
-    }
-  }
-
-  // cmdline::load (cmdline_hooks.cpp:50-96): relative paths resolve against
-  // the including config file's directory.
-  void load(const std::string& arg) {
-    std::string path = arg;
-    if (!dir_stack_.empty() && !path.empty() && path[0] != '/')
-      path = dir_stack_.back() + path;
-    if (exist("verbose")) std::cout << "# load: " << path << std::endl;
-    std::ifstream in(path);
-    if (!in.is_open()) throw "cannot open input config file: " + path;
-    const auto sep = path.find_last_of('/');
-    dir_stack_.push_back(sep == std::string::npos ? std::string() : path.substr(0, sep + 1));
-    std::vector<std::string> lines;
-    std::string line;
-    while (std::getline(in, line))
-      if (!line.empty() && line[0] != '#') lines.push_back(line);
-    const size_t n_rest = rest.size();
-    parse(lines, true);
-    rest.resize(n_rest);  // positional lines of a config file are ignored
-    dir_stack_.pop_back();
-  }
-
-  bool exist(const std::string& name) const { return opts_.at(name).count > 0; }
-  int count(const std::string& name) const { return opts_.at(name).count; }
-  std::string str(const std::string& name) const {
-    const Option& o = opts_.at(name);
-    return o.count ? o.value : o.def;
-  }
-  double num(const std::string& name) const {
-    const std::string s = str(name);
-    // vector options (--radius) keep their first comma-separated element
-    return std::strtod(s.substr(0, s.find(',')).c_str(), nullptr);
-  }
-  int integer(const std::string& name) const { return (int)std::strtol(str(name).c_str(), nullptr, 10); }
-  void set_int(const std::string& name, int v) {
-    Option& o = opts_.at(name);
-    o.value = std::to_string(v);
-    if (!o.count) o.count = 1;
-  }
-
-  std::string usage(const char* prog) const {
-    std::ostringstream os;
-    os << "usage: " << prog << " [options] ... response ...\n"
-       << "note: All length options below should be expressed in milimeters.\n"
-       << "options:\n";
-    for (const auto& name : order_) {
-      const Option& o = opts_.at(name);
-      os << "  ";
-      if (o.short_name) os << "-" << o.short_name << ", "; else os << "    ";
-      os << "--" << std::left << std::setw(16) << o.name << o.help;
-      if (o.has_value && !o.def.empty()) os << " (=" << o.def << ")";
-      os << "\n";
-    }
-    return os.str();
-  }
-
-  std::vector<std::string> rest;
-
- private:
-  void add(const std::string& name, char s, bool has_value, bool nff,
-           const std::string& def, const std::string& help) {
-    Option o;
-    o.name = name;
-    o.short_name = s;
-    o.has_value = has_value;
-    o.not_from_file = nff;
-    o.def = def;
-    o.help = help;
-    opts_[name] = o;
-    order_.push_back(name);
-  }
-  Option& get(const std::string& name) {
-    auto it = opts_.find(name);
-    if (it == opts_.end()) throw "undefined option: --" + name;
-    return it->second;
-  }
-  Option& get_short(char c) {
-    for (auto& kv : opts_)
-      if (kv.second.short_name == c) return kv.second;
-    throw std::string("undefined short option: -") + c;
-  }
-  void set(Option& o, const std::string& v, bool from_file) {
-    if (from_file && o.not_from_file) return;
-    if (o.name == "config") {
-      load(v);
-      return;
-    }
-    o.value = v;
-    ++o.count;
-  }
-
-  std::map<std::string, Option> opts_;
-  std::vector<std::string> order_;
-  std::vector<std::string> dir_stack_;
-};
-
-// path helpers (cmdline_types.h): extension, name without extension / path,
-// and add_index(index, max) -> "_<index>" zero-padded to the digits of max.
-std::string ext_of(const std::string& p) {
-  const auto sep = p.find_last_of("\\/"), dot = p.find_last_of('.');
-  if (dot == std::string::npos || (sep != std::string::npos && sep > dot)) return "";
-  return p.substr(dot);
-}
-std::string wo_ext(const std::string& p) { return p.substr(0, p.size() - ext_of(p).size()); }
-std::string wo_path(const std::string& p) {
-  const auto sep = p.find_last_of("\\/");
-  return sep == std::string::npos ? p : p.substr(sep + 1);
-}
-std::string add_index(const std::string& p, int index, int max) {
-  int digits = 1;
-  for (int m = 10; m <= max; m *= 10) ++digits;
-  std::ostringstream os;
-  os << p << "_" << std::setw(digits) << std::setfill('0') << index;
-  return os.str();
+// reconstruction_cmd.cpp:114-115 and options.cpp:44-76 on top of the shared
+// scanner options
+void add_reconstruction_options(Options& cl) {
+  cl.add_scanner_options();
+  cl.add("3d-response", 0, false, false, "", "input response contains additional LOR information");
+  cl.add("dl-is-time", 0, false, false, "", "delta is time, convert using speed of light");
+  cl.add("speed-of-light", 0, true, false, "299792458", "speed of light");
+  cl.add("scale-length", 0, true, false, "1", "scale input length values");
+  cl.add("scale-time", 0, true, false, "1", "scale input time values");
+  cl.add("blocks", 'i', true, false, "0", "number of iteration blocks");
+  cl.add("iterations", 'I', true, false, "1", "number of iterations (per block)");
+  cl.add("output", 'o', true, true, "", "output files prefix (png)");
+  cl.add("png-max", 0, true, false, "0", "maximum value mapped to 255 in PNG");
+  cl.add("gpu", 'G', false, false, "", "use the reference's GPU semantics");
+  cl.add("cuda-device", 'D', true, false, "0", "CUDA device");
+  cl.add("cuda-blocks", 'B', true, false, "64", "CUDA blocks (accepted, unused)");
+  cl.add("cuda-threads", 'W', true, false, "512", "CUDA threads per block (accepted, unused)");
+  cl.add("rho", 0, true, false, "", "start rho (eg. existing iteration)");
+  cl.add("rho-is-int", 0, false, false, "", "start rho uses integer representation (not float)");
+  cl.add("dump-responses", 0, true, true, "",
+         "write the responses as read (after unit conversion) to this binary file and exit");
 }
 
 // util::progress (util/progress.h:63-127) for -v (estimate) and -vv
@@ -293,6 +122,7 @@ int progress_cb(int completed, int finished, void* user) {
 
 int run(int argc, char** argv) {
   Options cl;
+  add_reconstruction_options(cl);
   std::vector<std::string> args(argv + 1, argv + argc);
   cl.parse(args, false);
   if (cl.exist("help")) {
@@ -300,15 +130,7 @@ int run(int argc, char** argv) {
     return 0;
   }
   // calculate_scanner_options (options.cpp:106-124), before the .cfg loading
-  if (cl.exist("n-pixels")) {
-    cl.set_int("n-z-pixels", cl.integer("n-pixels"));
-    cl.set_int("n-y-pixels", cl.integer("n-pixels"));
-  } else {
-    if (!cl.exist("n-z-pixels"))
-      cl.set_int("n-z-pixels", (int)std::ceil(cl.num("length") / cl.num("s-pixel")));
-    if (!cl.exist("n-y-pixels"))
-      cl.set_int("n-y-pixels", (int)std::ceil(2 * cl.num("radius") / cl.num("s-pixel")));
-  }
+  strip_cli::calculate_scanner_options(cl);
   if (cl.rest.empty()) {
     if (argc == 1) {
       std::cerr << cl.usage(argv[0]);

@@ -181,11 +181,11 @@ void write_raw(const std::string& path, const void* data, size_t bytes) {
 }
 
 void write_nrrd_header(const std::string& path, const std::string& data_file,
-                       int width, int height, bool textual) {
+                       int width, int height, bool textual, const char* type) {
   std::ofstream out(path);
   if (!out.is_open()) throw "cannot create output file: " + path;
   out << "NRRD0001" << std::endl
-      << "type: float" << std::endl
+      << "type: " << type << std::endl
       << "endian: little" << std::endl
       << "dimension: 2" << std::endl
       << "sizes: " << width << " " << height << std::endl

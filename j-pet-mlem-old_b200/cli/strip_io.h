@@ -14,6 +14,8 @@
 #pragma once
 
 #include <cstdint>
+#include <iomanip>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -29,9 +31,31 @@ void read_events_text(const std::string& path, bool is_3d,
 // One binary32 value with the reference fast parser's arithmetic; advances p.
 float parse_fp_reference(const char*& p);
 
+// path helpers (cmdline_types.h): extension, name without extension / path,
+// and add_index(index, max) -> "_<index>" zero-padded to the digits of max.
+inline std::string ext_of(const std::string& p) {
+  const auto sep = p.find_last_of("\\/"), dot = p.find_last_of('.');
+  if (dot == std::string::npos || (sep != std::string::npos && sep > dot)) return "";
+  return p.substr(dot);
+}
+inline std::string wo_ext(const std::string& p) { return p.substr(0, p.size() - ext_of(p).size()); }
+inline std::string wo_path(const std::string& p) {
+  const auto sep = p.find_last_of("\\/");
+  return sep == std::string::npos ? p : p.substr(sep + 1);
+}
+inline std::string add_index(const std::string& p, int index, int max) {
+  int digits = 1;
+  for (int m = 10; m <= max; m *= 10) ++digits;
+  std::ostringstream os;
+  os << p << "_" << std::setw(digits) << std::setfill('0') << index;
+  return os.str();
+}
+
 void write_raw(const std::string& path, const void* data, size_t bytes);
+// type: the NRRD element type ("float" for images, "int" for hit counts)
 void write_nrrd_header(const std::string& path, const std::string& data_file,
-                       int width, int height, bool textual);
+                       int width, int height, bool textual,
+                       const char* type = "float");
 // PixelMap text: values separated by ' ', '\n' after each row.
 void write_text_map(const std::string& path, const float* data, int width,
                     int height);

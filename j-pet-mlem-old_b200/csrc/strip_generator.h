@@ -54,12 +54,34 @@ STRIP_HD void philox(uint32_t ctr[4], uint32_t k0, uint32_t k1) {
 // (0, 1), never 0 or 1
 STRIP_HD double u01(uint32_t x) { return ((double)x + 0.5) * (1.0 / 4294967296.0); }
 
+// A phantom region (phantom.h:32-95): ellipse (axes a, b rotated by the
+// angle whose cosine / sine are c, s), rectangle (half sides a, b, not
+// rotated) or point; w = its weight, area x intensity (intensity alone for a
+// point).
 struct Region {
-  double z, y, a, b, c, s, w;  // centre, axes, cos/sin of the rotation, weight
+  int kind;  // STRIP_REGION_ELLIPSE / _RECTANGLE / _POINT
+  double z, y, a, b, c, s, w;
   STRIP_HD bool contains(double pz, double py) const {
     const double dz = pz - z, dy = py - y;
+    if (kind == STRIP_REGION_RECTANGLE) return fabs(dz) <= a && fabs(dy) <= b;
+    if (kind == STRIP_REGION_POINT) return pz == z && py == y;
     const double u = dz * c + dy * s, v = -dz * s + dy * c;
     return (u * u) / (a * a) + (v * v) / (b * b) <= 1.0;
+  }
+  // a point uniform in the region from two uniforms
+  STRIP_HD void point(double u1, double u2, double& pz, double& py) const {
+    if (kind == STRIP_REGION_RECTANGLE) {
+      pz = z + a * (2.0 * u1 - 1.0);
+      py = y + b * (2.0 * u2 - 1.0);
+    } else if (kind == STRIP_REGION_POINT) {
+      pz = z;
+      py = y;
+    } else {
+      const double rad = sqrt(u1), phi = 2.0 * kPi * u2;
+      const double lu = a * rad * cos(phi), lv = b * rad * sin(phi);
+      pz = z + lu * c - lv * s;
+      py = y + lu * s + lv * c;
+    }
   }
 };
 
@@ -69,21 +91,20 @@ struct Params {
   int uniform_angle;
 };
 
-// Emission from ellipses: r = region by cdf, point uniform in it, rejected
-// when an earlier region covers it.
-struct EllipseEmitter {
+// Emission from regions: r = region by cdf, point uniform in it; unless the
+// regions are additive, rejected when an earlier region covers the point
+// (phantom.h:193-204).
+struct RegionEmitter {
   const Region* reg;
   const double* cdf;
   int n;
+  int additive;
   STRIP_HD bool operator()(const uint32_t* c, double& pz, double& py) const {
     const double ur = u01(c[0]);
     int r = 0;
     while (r < n - 1 && ur > cdf[r]) ++r;
-    const Region& q = reg[r];
-    const double rad = sqrt(u01(c[1])), phi = 2.0 * kPi * u01(c[2]);
-    const double lu = q.a * rad * cos(phi), lv = q.b * rad * sin(phi);
-    pz = q.z + lu * q.c - lv * q.s;
-    py = q.y + lu * q.s + lv * q.c;
+    reg[r].point(u01(c[1]), u01(c[2]), pz, py);
+    if (additive) return true;
     for (int j = 0; j < r; ++j)
       if (reg[j].contains(pz, py)) return false;
     return true;
@@ -115,24 +136,40 @@ struct ImageEmitter {
 };
 
 // Event i: attempts (i, attempt) until an emission is detected, then the
-// smearing block (i, 0xFFFFFFFF, 1).  Returns false when kMaxAttempts
-// attempts all failed.
-template <class Emit>
-STRIP_HD bool event(const Params& p, uint64_t i, const Emit& emit, float& z_u,
-                    float& z_d, float& dl) {
+// smearing block (i, 0xFFFFFFFF, 1).  Returns kDetected, or kFailed when
+// kMaxAttempts attempts all failed.  With one_emission, event i is a single
+// emission (attempts only until a point is emitted, phantom.h:193-214) that
+// may go undetected (kEmitted).  on_emit(pz, py) sees every emission.
+enum EventStatus { kFailed = 0, kDetected = 1, kEmitted = 2 };
+
+struct NoEmitHook {
+  STRIP_HD void operator()(double, double) const {}
+};
+
+template <class Emit, class Hook = NoEmitHook>
+STRIP_HD int event(const Params& p, uint64_t i, const Emit& emit, float& z_u,
+                   float& z_d, float& dl, bool one_emission = false,
+                   double* origin = nullptr, const Hook& on_emit = Hook()) {
   const uint32_t ilo = (uint32_t)i, ihi = (uint32_t)(i >> 32);
   double pz = 0, py = 0, t = 0;
-  bool ok = false;
+  bool ok = false, emitted = false;
   for (uint32_t att = 0; att < kMaxAttempts && !ok; ++att) {
     uint32_t c[4] = {ilo, ihi, att, 0u};
     philox(c, p.k0, p.k1);
     if (!emit(c, pz, py)) continue;
+    emitted = true;
+    on_emit(pz, py);
     t = p.uniform_angle ? tan(kPi * (u01(c[3]) - 0.5))
                         : p.tmax * (2.0 * u01(c[3]) - 1.0);
     const double zu = pz + (p.R - py) * t, zd = pz - (p.R + py) * t;
     ok = fabs(zu) < p.hL && fabs(zd) < p.hL;
+    if (one_emission) break;
   }
-  if (!ok) return false;
+  if (origin) {
+    origin[0] = pz;
+    origin[1] = py;
+  }
+  if (!ok) return emitted && one_emission ? kEmitted : kFailed;
   uint32_t c[4] = {ilo, ihi, 0xFFFFFFFFu, 1u};
   philox(c, p.k0, p.k1);
   // Box-Muller: two normal pairs from four uniforms
@@ -145,12 +182,14 @@ STRIP_HD bool event(const Params& p, uint64_t i, const Emit& emit, float& z_u,
   z_u = (float)(zu + p.sigma_z * n0);
   z_d = (float)(zd + p.sigma_z * n1);
   dl = (float)(d + p.sigma_dl * n2);
-  return true;
+  return kDetected;
 }
 
 // Host-side set-up shared by both generators (strip_phantom.cpp).
 Params make_params(const strip_geometry* g, uint64_t seed, int uniform_angle);
 bool make_regions(const strip_ellipse* el, int n_el, std::vector<Region>& reg,
+                  std::vector<double>& cdf);
+bool make_regions(const strip_region* rg, int n_rg, std::vector<Region>& reg,
                   std::vector<double>& cdf);
 bool make_image_cdf(const strip_geometry* g, const float* rho,
                     std::vector<double>& cdf);

@@ -21,7 +21,9 @@ int generate(const stripgen::Params& p, int64_t n, float* z_u, float* z_d,
   int bad = 0;
 #pragma omp parallel for schedule(static, 4096) reduction(| : bad)
   for (int64_t i = 0; i < n; ++i)
-    if (!stripgen::event(p, (uint64_t)i, emit, z_u[i], z_d[i], dl[i])) bad = 1;
+    if (stripgen::event(p, (uint64_t)i, emit, z_u[i], z_d[i], dl[i]) !=
+        stripgen::kDetected)
+      bad = 1;
   return bad ? STRIP_E_INVALID : STRIP_OK;
 }
 
@@ -44,22 +46,52 @@ Params make_params(const strip_geometry* g, uint64_t seed, int uniform_angle) {
 
 // Regions and their cumulative weights (area x activity); false when an
 // ellipse is invalid or the total weight is zero.
-bool make_regions(const strip_ellipse* el, int n_el, std::vector<Region>& reg,
+bool make_regions(const strip_region* rg, int n_rg, std::vector<Region>& reg,
                   std::vector<double>& cdf) {
-  reg.resize((size_t)n_el);
-  cdf.resize((size_t)n_el);
+  reg.resize((size_t)n_rg);
+  cdf.resize((size_t)n_rg);
   double acc = 0;
-  for (int i = 0; i < n_el; ++i) {
-    if (!(el[i].a > 0) || !(el[i].b > 0) || !(el[i].activity >= 0)) return false;
-    const double ang = el[i].angle_deg * kPi / 180.0;
-    reg[i] = Region{el[i].z, el[i].y, el[i].a, el[i].b, std::cos(ang),
-                    std::sin(ang), kPi * el[i].a * el[i].b * el[i].activity};
-    acc += reg[i].w;
+  for (int i = 0; i < n_rg; ++i) {
+    const strip_region& q = rg[i];
+    if (!(q.intensity >= 0) || !std::isfinite(q.z) || !std::isfinite(q.y)) return false;
+    Region r{};
+    r.kind = q.kind;
+    r.z = q.z;
+    r.y = q.y;
+    if (q.kind == STRIP_REGION_ELLIPSE) {
+      if (!(q.a > 0) || !(q.b > 0)) return false;
+      const double ang = q.angle_deg * kPi / 180.0;
+      r.a = q.a;
+      r.b = q.b;
+      r.c = std::cos(ang);
+      r.s = std::sin(ang);
+      r.w = kPi * q.a * q.b * q.intensity;
+    } else if (q.kind == STRIP_REGION_RECTANGLE) {
+      if (!(q.a > 0) || !(q.b > 0)) return false;
+      r.a = q.a;
+      r.b = q.b;
+      r.w = 4.0 * q.a * q.b * q.intensity;
+    } else if (q.kind == STRIP_REGION_POINT) {
+      r.w = q.intensity;
+    } else {
+      return false;
+    }
+    reg[i] = r;
+    acc += r.w;
     cdf[i] = acc;
   }
   if (!(acc > 0)) return false;
   for (auto& c : cdf) c /= acc;
   return true;
+}
+
+bool make_regions(const strip_ellipse* el, int n_el, std::vector<Region>& reg,
+                  std::vector<double>& cdf) {
+  std::vector<strip_region> rg((size_t)n_el);
+  for (int i = 0; i < n_el; ++i)
+    rg[i] = strip_region{STRIP_REGION_ELLIPSE, 0, el[i].z, el[i].y, el[i].a,
+                         el[i].b, el[i].angle_deg, el[i].activity};
+  return make_regions(rg.data(), n_el, reg, cdf);
 }
 
 // Cumulative pixel weights of an activity image; false when a pixel is
@@ -110,7 +142,7 @@ extern "C" int strip_generate_events(const strip_geometry* g,
   std::vector<stripgen::Region> reg;
   std::vector<double> cdf;
   if (!stripgen::make_regions(el, n_el, reg, cdf)) return STRIP_E_INVALID;
-  const stripgen::EllipseEmitter emit{reg.data(), cdf.data(), n_el};
+  const stripgen::RegionEmitter emit{reg.data(), cdf.data(), n_el, 0};
   return generate(stripgen::make_params(g, seed, 0), n, z_u, z_d, dl, emit);
 }
 

@@ -48,6 +48,24 @@ class Geometry(ctypes.Structure):
     ]
 
 
+REGION_ELLIPSE, REGION_RECTANGLE, REGION_POINT = 0, 1, 2
+
+
+class Region(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("z", ctypes.c_double), ("y", ctypes.c_double), ("a", ctypes.c_double),
+                ("b", ctypes.c_double), ("angle_deg", ctypes.c_double),
+                ("intensity", ctypes.c_double)]
+
+
+class Simulation(ctypes.Structure):
+    _fields_ = [("additive", ctypes.c_int32), ("uniform_angle", ctypes.c_int32),
+                ("count_emitted", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("d_emitted", ctypes.c_void_p), ("d_detected", ctypes.c_void_p),
+                ("pixel_size", ctypes.c_double), ("origin_z", ctypes.c_double),
+                ("origin_y", ctypes.c_double)]
+
+
 class Tuning(ctypes.Structure):
     _fields_ = [("tile", ctypes.c_int32), ("grab", ctypes.c_int32), ("ms", ctypes.c_double)]
 
@@ -173,6 +191,18 @@ SIGNATURES = {
         ctypes.c_int,
         [_P(Geometry), _f, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int,
          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
+    "strip_simulate_device": (
+        ctypes.c_int,
+        [_P(Geometry), _P(Region), ctypes.c_int, _P(Simulation), ctypes.c_uint64,
+         ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+         _P(ctypes.c_int64), _P(ctypes.c_int64)],
+    ),
+    "strip_simulate": (
+        ctypes.c_int,
+        [_P(Geometry), _P(Region), ctypes.c_int, _P(Simulation), ctypes.c_uint64,
+         ctypes.c_int64, ctypes.c_int, _f, _f, _f, _P(ctypes.c_uint32), _P(ctypes.c_uint32),
+         _P(ctypes.c_int64), _P(ctypes.c_int64)],
     ),
     "strip_generate_events_image": (
         ctypes.c_int,

@@ -12,8 +12,10 @@ from conftest import PKG, ROOT
 from oracle import oracle as orc
 
 CLI = os.path.join(PKG, "bin", "2d_strip_reconstruction")
+PHANTOM_CLI = os.path.join(PKG, "bin", "2d_strip_phantom")
 GOLD = os.path.join(ROOT, "tests", "golden")
 C1_ARGS = ["-r", "200", "-l", "500", "-p", "2", "--s-z", "10", "--s-dl", "42"]
+C1_PHANTOM_T = [(40, 30, 30, 20, 0, 3.0), (-50, -20, 25, 40, 0, 0.3), (0, 0, 150, 100, 0, 1.0)]
 
 
 def run_cli(*args, cwd=None, check=True):
@@ -125,3 +127,82 @@ def test_gpu_semantics_output_schedule(tmp_path):
     img = np.fromfile(tmp_path / "g_6.bin", dtype="<f4").reshape(200, 250)
     r64 = orc.mlem_f64(g, ev[:, 0], ev[:, 1], ev[:, 2], 6, mode=orc.MODE_GPU)
     assert np.linalg.norm(img - r64) / np.linalg.norm(r64) < 1e-4
+
+
+def run_phantom(*args, cwd=None, check=True):
+    p = subprocess.run([PHANTOM_CLI, *map(str, args)], capture_output=True, text=True,
+                       cwd=cwd, timeout=600)
+    if check and p.returncode != 0:
+        raise AssertionError(f"phantom CLI failed ({p.returncode}): {p.stderr}")
+    return p
+
+
+def test_phantom_cli_options_and_errors(tmp_path):
+    p = run_phantom("--help")
+    for opt in ("--scale", "--additive", "--detected", "--point", "--image-origin",
+                "--n-emissions", "--output", "--s-z", "--s-dl", "--seed"):
+        assert opt in p.stderr, opt
+    bad = tmp_path / "bad"
+    bad.write_text("ellipse 0 0 10 10 0 1\ntriangle 0 0 1\n")
+    p = run_phantom(bad, "-e", "10", "-o", tmp_path / "x.bin", check=False)
+    assert p.returncode == 1 and "unknown phantom type: triangle" in p.stderr
+
+
+@pytest.mark.gpu
+def test_phantom_cli_detected_stream_matches_generator(tmp_path):
+    """--detected --uniform-tan with ellipses is the library's generator:
+    the same events as stripmlem.generate_events for the same seed."""
+    import stripmlem as sm
+    ph = tmp_path / "c1_phantom"
+    ph.write_text("".join(f"ellipse {z} {y} {a} {b} {ang} {act}\n"
+                          for z, y, a, b, ang, act in C1_PHANTOM_T))
+    out = tmp_path / "p.bin"
+    p = run_phantom(ph, *C1_ARGS, "-e", "20k", "--detected", "--uniform-tan", "--seed", "7",
+                    "-o", out, "-v")
+    assert "detected: 20000 events" in p.stderr
+    ev = np.fromfile(out, dtype="<f4").reshape(-1, 3)
+    sc = sm.Scanner(200.0, 500.0, 200, 250, 2.0, 2.0, 10.0, 42.0)
+    ref = np.stack(sm.generate_events(sc, C1_PHANTOM_T, 20000, seed=7), 1)
+    same = np.all(ev.view(np.uint32) == ref.view(np.uint32), axis=1)
+    assert same.mean() >= 1 - 1e-4
+    cfg = (tmp_path / "p.cfg").read_text()
+    for line in ("--radius=200", "--length=500", "--s-pixel=2", "--s-z=10", "--s-dl=42",
+                 "--n-z-pixels=250", "--n-y-pixels=200"):
+        assert line in cfg, (line, cfg)
+    det = np.fromfile(tmp_path / "p_detected", dtype="<i4").reshape(200, 250)
+    assert det.sum() == 20000  # every emission point lies on the image grid
+    emi = np.fromfile(tmp_path / "p_emitted", dtype="<i4").reshape(200, 250)
+    assert emi.sum() > det.sum()
+    naive = np.fromfile(tmp_path / "p_naive", dtype="<i4").reshape(200, 250)
+    assert 0.9 * 20000 < naive.sum() <= 20000
+    assert "type: int" in (tmp_path / "p_detected.nrrd").read_text()
+    # the reconstruction reads the accompanying .cfg
+    r = run_cli(out, "-i", "1", "-I", "2", "-o", tmp_path / "r.bin", "-v")
+    img = np.fromfile(tmp_path / "r_2.bin", dtype="<f4").reshape(200, 250)
+    assert np.isfinite(img).all() and img.sum() > 0
+
+
+@pytest.mark.gpu
+def test_phantom_cli_emissions_and_shapes(tmp_path):
+    ph = tmp_path / "shapes"
+    ph.write_text("rectangle 0 0 60 40 1\nellipse 30 10 20 10 30 2\npoint 10 20 5000\n"
+                  "ellipse 1 2 3\nellipse 0 0 100 100 0 1\n")  # the malformed line ends the file
+    out = tmp_path / "e.txt"
+    p = run_phantom(ph, *C1_ARGS, "-e", "30000", "--additive", "-o", out, "-v",
+                    "--scale", "2")
+    assert " emitted: 30000 events" in p.stderr
+    lines = out.read_text().splitlines()
+    n_det = int(p.stderr.split("detected:")[1].split()[0])
+    assert len(lines) == n_det and 0 < n_det < 30000
+    assert len(lines[0].split()) == 3
+    emi = np.fromfile(tmp_path / "e_emitted", dtype="<i4").reshape(200, 250)
+    # scale 2: the rectangle spans |z| <= 120, |y| <= 80 mm; nothing outside
+    rows = np.nonzero(emi.sum(1))[0]
+    cols = np.nonzero(emi.sum(0))[0]
+    assert cols.min() >= 125 - 60 - 1 and cols.max() <= 125 + 60
+    assert rows.min() >= 100 - 40 - 1 and rows.max() <= 100 + 40
+    # the point source (not scaled) holds its share: weight 5000 vs 4*120*80 + pi*40*20*2
+    total_w = 4 * 120 * 80 + np.pi * 40 * 20 * 2 + 5000
+    z, y = 10.0, 20.0
+    col, row = int(np.floor((z + 250) / 2)), int(np.floor((y + 200) / 2))
+    assert emi[row, col] > 0.8 * 30000 * 5000 / total_w
