@@ -99,6 +99,18 @@ __device__ __forceinline__ unsigned to_fixed(float x, float s) {
   return __float_as_uint(fmaf(x, s, kMagic)) - kMagicBits;
 }
 
+// Shared-memory access by 32-bit shared-space byte address: the walks below
+// advance one address register per step and let the loads and atomics use
+// immediate offsets.
+__device__ __forceinline__ float lds32(uint32_t addr) {
+  float v;
+  asm("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+  return v;
+}
+__device__ __forceinline__ void red_shared_add(uint32_t addr, unsigned v) {
+  asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
 // How a shared-memory window accumulates the backprojection:
 //   kAccF32     binary32 atomics (a load and a compare-and-swap per add here)
 //   kAccU32     unsigned fixed point, the 2^23 addend (rho-weighted MLEM)
@@ -114,6 +126,10 @@ struct SmemWin {
   float* acc;
   int wx0, wy0, WS;
   float fixed_unit;
+  uint32_t w_sh, acc_sh;  // shared-space addresses of w and acc
+  static constexpr bool kShared = true;
+  __device__ __forceinline__ uint32_t w_addr(int p) const { return w_sh + 4u * (uint32_t)p; }
+  __device__ __forceinline__ uint32_t acc_addr(int p) const { return acc_sh + 4u * (uint32_t)p; }
   __device__ __forceinline__ float unit() const {
     return KIND == kAccF32 ? 1.0f : fixed_unit;
   }
@@ -145,6 +161,7 @@ struct SmemWin {
     atomicAdd(ai, (int)(__float_as_uint(x.x) - kMagicSignedBits));
     atomicAdd(ai + 1, (int)(__float_as_uint(x.y) - kMagicSignedBits));
   }
+  __host__ __device__ static constexpr bool fine() { return KIND == kAccU32Cvt; }
   // the same for pixels j, j + 1 with K = P * pref (packed)
   __host__ __device__ static constexpr bool pair_scatter() {
     return KIND == kAccU32 || KIND == kAccU32Cvt;
@@ -188,6 +205,9 @@ struct GlobalWin {
     atomicAdd(acc + p + j, (double)v);
   }
   __device__ __forceinline__ float unit() const { return 1.0f; }
+  static constexpr bool kShared = false;
+  __device__ __forceinline__ uint32_t w_addr(int64_t) const { return 0; }
+  __device__ __forceinline__ uint32_t acc_addr(int64_t) const { return 0; }
   __host__ __device__ static constexpr bool pair_scatter() { return false; }
   __host__ __device__ static constexpr bool pair_add() { return false; }
   __device__ __forceinline__ void add2(int64_t, int, f32x2, float) const {}
@@ -317,7 +337,25 @@ __device__ __forceinline__ void pass1_rows(const ScannerF& s, const KernelF& k,
       const auto p = win.ptr(e.tly + ranked_row(H, rank0 + 32 * b + lane),
                              run_lo(L.lolen[b]));
       float a = 0.0f;
-      if constexpr (MODE == STRIP_MODE_CPU && kPairs) {
+      if constexpr (MODE == STRIP_MODE_CPU && kPairs && Win::kShared) {
+        // two pixels per step: a count-down loop over pairs, one shared
+        // address register, float2 arithmetic
+        const float E0 = L.E0[b], R0 = L.R0[b], R2 = R0 * R0;
+        float2 P = make_float2(E0, E0 * R0);
+        float2 S = make_float2(R2 * k.q, R2 * k.q3);
+        const float2 Q4 = make_float2(k.q4, k.q4);
+        float2 A = make_float2(0.0f, 0.0f);
+        uint32_t ad = win.w_addr(p);
+#pragma unroll 2
+        for (int c = n >> 1; c > 0; --c, ad += 8) {
+          A = __ffma2_rn(P, make_float2(lds32(ad), lds32(ad + 4)), A);
+          P = __fmul2_rn(P, S);
+          S = __fmul2_rn(S, Q4);
+        }
+        a = A.x + A.y;
+        if (n & 1) a = fmaf(P.x, lds32(ad), a);
+        acc.add(L.pref[b] * a);
+      } else if constexpr (MODE == STRIP_MODE_CPU && kPairs) {
         PairRecurrence g(k, L.E0[b], L.R0[b]);
         f32x2 A = pack2(0.0f, 0.0f);
 #pragma unroll 2
@@ -369,6 +407,39 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
       const auto p = win.ptr(e.tly + ranked_row(H, rank0 + 32 * b + lane),
                              run_lo(L.lolen[b]));
       if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED && kPairs &&
+                    Win::pair_scatter() && Win::kShared) {
+        // pass 1's walk (the same K values to the bit), u = K w / D in fixed
+        // point with native shared integer reductions
+        const float E0 = L.E0[b], R0 = L.R0[b], R2 = R0 * R0;
+        float2 P = make_float2(E0, E0 * R0);
+        float2 S = make_float2(R2 * k.q, R2 * k.q3);
+        const float2 Q4 = make_float2(k.q4, k.q4);
+        const float sc = fminf(L.pref[b] * scale * win.unit(), 3.0e38f);
+        const float2 SC = make_float2(sc, sc);
+        uint32_t ad = win.w_addr(p), aa = win.acc_addr(p);
+#pragma unroll 2
+        for (int c = n >> 1; c > 0; --c, ad += 8, aa += 8) {
+          const float2 kw = __fmul2_rn(P, make_float2(lds32(ad), lds32(ad + 4)));
+          unsigned v0, v1;
+          if constexpr (Win::fine()) {
+            const float2 x = __fmul2_rn(kw, SC);
+            v0 = __float2uint_rn(x.x);
+            v1 = __float2uint_rn(x.y);
+          } else {
+            const float2 x = __ffma2_rn(kw, SC, make_float2(kMagic, kMagic));
+            v0 = __float_as_uint(x.x) - kMagicBits;
+            v1 = __float_as_uint(x.y) - kMagicBits;
+          }
+          red_shared_add(aa, v0);
+          red_shared_add(aa + 4, v1);
+          P = __fmul2_rn(P, S);
+          S = __fmul2_rn(S, Q4);
+        }
+        if (n & 1) {
+          const float kw = P.x * lds32(ad);
+          red_shared_add(aa, Win::fine() ? __float2uint_rn(kw * sc) : to_fixed(kw, sc));
+        }
+      } else if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED && kPairs &&
                     Win::pair_scatter()) {
         PairRecurrence g(k, L.E0[b], L.R0[b]);
         const float sc = fminf(L.pref[b] * scale * win.unit(), 3.0e38f);
@@ -637,22 +708,24 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
     fshift = adjoint_shift(a, it, lane);
   }
   const float unit = exp2f((float)fshift);
+  const uint32_t w_sh = (uint32_t)__cvta_generic_to_shared(s_w);
+  const uint32_t acc_sh = (uint32_t)__cvta_generic_to_shared(s_acc);
   if constexpr (OP == OP_MLEM && MODE == STRIP_MODE_CPU) {
     if (fshift > 22)
       run_item<OP, MODE, ACC>(
-          a, it, SmemWin<kAccU32Cvt>{s_w, s_acc, wx0, wy0, WS, unit}, lane,
+          a, it, SmemWin<kAccU32Cvt>{s_w, s_acc, wx0, wy0, WS, unit, w_sh, acc_sh}, lane,
           s_next_group);
     else
       run_item<OP, MODE, ACC>(
-          a, it, SmemWin<kAccU32>{s_w, s_acc, wx0, wy0, WS, unit}, lane,
+          a, it, SmemWin<kAccU32>{s_w, s_acc, wx0, wy0, WS, unit, w_sh, acc_sh}, lane,
           s_next_group);
   } else if constexpr (OP == OP_ADJOINT && MODE == STRIP_MODE_CPU) {
     run_item<OP, MODE, ACC>(a, it,
-                            SmemWin<kAccS32>{s_w, s_acc, wx0, wy0, WS, unit},
+                            SmemWin<kAccS32>{s_w, s_acc, wx0, wy0, WS, unit, w_sh, acc_sh},
                             lane, s_next_group);
   } else {
     run_item<OP, MODE, ACC>(a, it,
-                            SmemWin<kAccF32>{s_w, s_acc, wx0, wy0, WS, 1.0f},
+                            SmemWin<kAccF32>{s_w, s_acc, wx0, wy0, WS, 1.0f, w_sh, acc_sh},
                             lane, s_next_group);
   }
   if (kWrites) {
