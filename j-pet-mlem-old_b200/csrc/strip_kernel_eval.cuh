@@ -115,6 +115,35 @@ struct GaussRow {
   }
 };
 
+// GaussianKernel row constants from three per-event ones.  With yp = dy + y,
+//   a'Sa = ipsz sec^4 ((yp - R)^2 + (yp + R)^2) + ipsdl (2 yp sec tan)^2
+//        = na yp^2 + nb,    na = 2 ipsz sec^4 + 4 ipsdl sec^2 tan^2,
+//                           nb = 2 ipsz sec^4 R^2,
+// and the row's part of the exponent, -log2(e)/2 * ipsdl (2 dy sec)^2, is
+// cd dy^2 with cd = -2 log2(e) ipsdl sec^2 (the same values as GaussRow up
+// to rounding, for a third of its arithmetic).
+struct GaussEvent {
+  float na, nb, cd;
+  __device__ __forceinline__ void init(const KernelF& k, float R, float tan,
+                                       float sec) {
+    const float s2 = sec * sec, s4 = s2 * s2;
+    na = 2.0f * k.ipsz * s4 + 4.0f * k.ipsdl * s2 * (tan * tan);
+    nb = 2.0f * k.ipsz * s4 * (R * R);
+    cd = -2.0f * kLog2e * k.ipsdl * s2;
+  }
+  // K and the recurrence ratio R at the run's first pixel, whose distance
+  // from the event along z is t0 (so t = t0 - dy tan).
+  __device__ __forceinline__ void row(const KernelF& k, float y, float tan,
+                                      float dy, float t0, float& K0,
+                                      float& R0) const {
+    const float yp = dy + y;
+    const float pref = k.kc * rsqrt_approx(fmaf(na, yp * yp, nb));
+    const float t = fmaf(-dy, tan, t0);
+    K0 = pref * ex2_approx(fmaf(k.c1 * t, t, cd * dy * dy));
+    R0 = ex2_approx(fmaf(k.r1, t, k.r0));
+  }
+};
+
 // GaussianKernel row with the sigma derivatives of log K.  With
 // N = a'Sa = ipsz a_pq + ipsdl a_r^2 (a_pq = ap^2 + aq^2) and kc ~ 1/(sz^2 sdl):
 //   sz  * dlogK/dsz  = -2 + ipsz a_pq / N + 2 ipsz t^2   = fz  + 2 ipsz t^2

@@ -111,6 +111,13 @@ __device__ __forceinline__ void red_shared_add(uint32_t addr, unsigned v) {
   asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
 
+// Row of rank i among an event's H box rows, ranked middle-out: the centre
+// row first, then alternately below and above.
+__device__ __forceinline__ int ranked_row(int H, int i) {
+  const int mid = (H - 1) >> 1;
+  return mid + ((i & 1) ? ((i + 1) >> 1) : -(i >> 1));
+}
+
 // How a shared-memory window accumulates the backprojection:
 //   kAccF32     binary32 atomics (a load and a compare-and-swap per add here)
 //   kAccU32     unsigned fixed point, the 2^23 addend (rho-weighted MLEM)
@@ -136,6 +143,15 @@ struct SmemWin {
   __device__ __forceinline__ int ptr(int iy, int col) const {
     return (iy - wy0) * WS + (col - wx0);
   }
+  // A lane's run of row iy kept in one register: window offset << 16 | len
+  // (windows hold < 2^15 pixels, runs < 2^16).
+  __device__ __forceinline__ unsigned pack_run(int iy, int lo, int len) const {
+    return len > 0 ? ((unsigned)ptr(iy, lo) << 16) | (unsigned)len : 0u;
+  }
+  __device__ __forceinline__ int run_ptr(unsigned v, const EventF&, int,
+                                         int) const {
+    return (int)(v >> 16);
+  }
   __device__ __forceinline__ float read(int p, int j) const { return w[p + j]; }
   // acc_j += v (v already scaled by unit())
   __device__ __forceinline__ void add(int p, int j, float v) const {
@@ -152,37 +168,12 @@ struct SmemWin {
                                           : to_fixed(E * w[p + j], sc);
     atomicAdd(reinterpret_cast<unsigned*>(acc) + p + j, v);
   }
-  // acc_j += P.x * sc, acc_j+1 += P.y * sc (signed fixed point)
+  // signed fixed point: the adjoint's pair walk adds two pixels a step
   __host__ __device__ static constexpr bool pair_add() { return KIND == kAccS32; }
-  __device__ __forceinline__ void add2(int p, int j, f32x2 P, float sc) const {
-    const float2 x = unpack2(fma2(P, pack2(sc, sc),
-                                  pack2(kMagicSigned, kMagicSigned)));
-    int* ai = reinterpret_cast<int*>(acc) + p + j;
-    atomicAdd(ai, (int)(__float_as_uint(x.x) - kMagicSignedBits));
-    atomicAdd(ai + 1, (int)(__float_as_uint(x.y) - kMagicSignedBits));
-  }
   __host__ __device__ static constexpr bool fine() { return KIND == kAccU32Cvt; }
-  // the same for pixels j, j + 1 with K = P * pref (packed)
+  // the rho-weighted MLEM scatter takes two pixels a step
   __host__ __device__ static constexpr bool pair_scatter() {
     return KIND == kAccU32 || KIND == kAccU32Cvt;
-  }
-  __device__ __forceinline__ void add_weighted2(int p, int j, f32x2 P,
-                                                float sc) const {
-    unsigned* au = reinterpret_cast<unsigned*>(acc) + p + j;
-    const f32x2 kw = mul2(P, pack2(w[p + j], w[p + j + 1]));
-    unsigned v0, v1;
-    if constexpr (KIND == kAccU32Cvt) {
-      const float2 x = unpack2(mul2(kw, pack2(sc, sc)));
-      v0 = __float2uint_rn(x.x);
-      v1 = __float2uint_rn(x.y);
-    } else {
-      const float2 x =
-          unpack2(fma2(kw, pack2(sc, sc), pack2(kMagic, kMagic)));
-      v0 = __float_as_uint(x.x) - kMagicBits;
-      v1 = __float_as_uint(x.y) - kMagicBits;
-    }
-    atomicAdd(au, v0);
-    atomicAdd(au + 1, v1);
   }
 };
 
@@ -195,6 +186,14 @@ struct GlobalWin {
   int n_z;
   __device__ __forceinline__ int64_t ptr(int iy, int col) const {
     return (int64_t)iy * n_z + col;
+  }
+  // lo << 16 | len; the row is recomputed from the lane's rank
+  __device__ __forceinline__ unsigned pack_run(int, int lo, int len) const {
+    return len > 0 ? ((unsigned)lo << 16) | (unsigned)len : 0u;
+  }
+  __device__ __forceinline__ int64_t run_ptr(unsigned v, const EventF& e,
+                                             int H, int rank) const {
+    return ptr(e.tly + ranked_row(H, rank), (int)(v >> 16));
   }
   __device__ __forceinline__ float read(int64_t p, int j) const {
     float v = __ldg(rho + p + j);
@@ -210,7 +209,6 @@ struct GlobalWin {
   __device__ __forceinline__ uint32_t acc_addr(int64_t) const { return 0; }
   __host__ __device__ static constexpr bool pair_scatter() { return false; }
   __host__ __device__ static constexpr bool pair_add() { return false; }
-  __device__ __forceinline__ void add2(int64_t, int, f32x2, float) const {}
   __device__ __forceinline__ void add_weighted(int64_t p, int j, float E,
                                                float sc) const {
     atomicAdd(acc + p + j, (double)(E * read(p, j) * sc));
@@ -242,8 +240,8 @@ __device__ __forceinline__ void walk_share(const RowTables& T, int nrows,
 // middle-out (the centre row first, then alternately below and above), so a
 // block of 32 consecutive ranks holds rows of similar run length; lane l of
 // block k owns the row of rank 32k + l.  A lane keeps its rows' run (lo, len)
-// and recurrence state (E0, R0, pref) in registers across both passes: pass 1
-// walks its runs with E <- E*R, R <- R*q (no per-pixel exponential, no
+// and recurrence state (K0, R0) in registers across both passes: pass 1
+// walks its runs with K <- K*R, R <- R*q (no per-pixel exponential, no
 // per-pixel bookkeeping), pass 2 walks them again from the stored state.
 // Events with more than kRowBlocks*32 rows are processed in super-blocks and
 // rebuilt for pass 2.
@@ -255,59 +253,50 @@ constexpr int kRowBlocks = 3;
 #endif
 constexpr bool kPairs = STRIP_PAIRS != 0;
 
-__device__ __forceinline__ int ranked_row(int H, int i) {
-  const int mid = (H - 1) >> 1;
-  return mid + ((i & 1) ? ((i + 1) >> 1) : -(i >> 1));
-}
-
 template <int MODE>
 struct LaneRows;
 
-// Run of block b: lolen[b] = lo << 16 | len (len == 0: no run).
-__device__ __forceinline__ int run_lo(int v) { return v >> 16; }
-__device__ __forceinline__ int run_len(int v) { return v & 0xFFFF; }
+// Run of block b: run[b] = the window's packed run (len == 0: no run).
+__device__ __forceinline__ int run_len(unsigned v) { return (int)(v & 0xFFFFu); }
 
-// GaussianKernel: K = pref * E along the run, E(t0) = 2^(c1 t0^2 + c0)
+// GaussianKernel: K along the run from K0 = K(t0) and the ratio R0
 template <>
 struct LaneRows<STRIP_MODE_CPU> {
-  int lolen[kRowBlocks];
-  float E0[kRowBlocks], R0[kRowBlocks], pref[kRowBlocks];
+  unsigned run[kRowBlocks];
+  float K0[kRowBlocks], R0[kRowBlocks];
 };
 // AnalyticKernel: direct evaluation per pixel from the row constants
 template <>
 struct LaneRows<STRIP_MODE_GPU> {
-  int lolen[kRowBlocks];
+  unsigned run[kRowBlocks];
   float t0[kRowBlocks], n0[kRowBlocks], n1[kRowBlocks], u0[kRowBlocks],
       u1[kRowBlocks], cr[kRowBlocks];
 };
 
 // Builds the lane's rows of ranks [rank0, rank0 + 32*kRowBlocks).
-template <int MODE>
+template <int MODE, class Win>
 __device__ __forceinline__ void build_lane_rows(const ScannerF& s,
                                                 const KernelF& k,
                                                 const EventF& e,
-                                                const EventRows& er, int H,
+                                                const EventRows& er,
+                                                const GaussEvent& ge, int H,
                                                 int rank0, int lane,
+                                                const Win& win,
                                                 LaneRows<MODE>& L) {
 #pragma unroll
   for (int b = 0; b < kRowBlocks; ++b) {
-    L.lolen[b] = 0;
+    L.run[b] = 0u;
     const int i = rank0 + 32 * b + lane;
     if (i < H) {
       const int iy = e.tly + ranked_row(H, i);
       const RowSet rs = row_set(s, e, iy);
       int lo;
       const int len = row_run(s, e, er, rs, lo);
-      L.lolen[b] = (lo << 16) | len;
+      L.run[b] = win.pack_run(iy, lo, len);
       if (len > 0) {
         const float t0 = (fmaf((float)lo, s.pw, s.tl_z_half_w) - e.z);
         if constexpr (MODE == STRIP_MODE_CPU) {
-          GaussRow g;
-          g.init(k, s.R, e.y, e.tan, e.sec, rs.dy);
-          const float t = t0 - g.dytan;
-          L.E0[b] = ex2_approx(fmaf(k.c1 * t, t, g.c0));
-          L.R0[b] = ex2_approx(fmaf(k.r1, t, k.r0));
-          L.pref[b] = g.pref;
+          ge.row(k, e.y, e.tan, rs.dy, t0, L.K0[b], L.R0[b]);
         } else {
           AnalyticRow g;
           g.init(k, s.R, e.y, e.tan, e.sec, rs.dy);
@@ -332,16 +321,15 @@ __device__ __forceinline__ void pass1_rows(const ScannerF& s, const KernelF& k,
                                            RowSum<ACC>& acc) {
 #pragma unroll
   for (int b = 0; b < kRowBlocks; ++b) {
-    const int n = run_len(L.lolen[b]);
+    const int n = run_len(L.run[b]);
     if (b < nb && n > 0) {
-      const auto p = win.ptr(e.tly + ranked_row(H, rank0 + 32 * b + lane),
-                             run_lo(L.lolen[b]));
+      const auto p = win.run_ptr(L.run[b], e, H, rank0 + 32 * b + lane);
       float a = 0.0f;
       if constexpr (MODE == STRIP_MODE_CPU && kPairs && Win::kShared) {
         // two pixels per step: a count-down loop over pairs, one shared
         // address register, float2 arithmetic
-        const float E0 = L.E0[b], R0 = L.R0[b], R2 = R0 * R0;
-        float2 P = make_float2(E0, E0 * R0);
+        const float K0 = L.K0[b], R0 = L.R0[b], R2 = R0 * R0;
+        float2 P = make_float2(K0, K0 * R0);
         float2 S = make_float2(R2 * k.q, R2 * k.q3);
         const float2 Q4 = make_float2(k.q4, k.q4);
         float2 A = make_float2(0.0f, 0.0f);
@@ -354,9 +342,8 @@ __device__ __forceinline__ void pass1_rows(const ScannerF& s, const KernelF& k,
         }
         a = A.x + A.y;
         if (n & 1) a = fmaf(P.x, lds32(ad), a);
-        acc.add(L.pref[b] * a);
       } else if constexpr (MODE == STRIP_MODE_CPU && kPairs) {
-        PairRecurrence g(k, L.E0[b], L.R0[b]);
+        PairRecurrence g(k, L.K0[b], L.R0[b]);
         f32x2 A = pack2(0.0f, 0.0f);
 #pragma unroll 2
         for (int j = 0; j + 1 < n; j += 2) {
@@ -366,16 +353,14 @@ __device__ __forceinline__ void pass1_rows(const ScannerF& s, const KernelF& k,
         const float2 a2 = unpack2(A);
         a = a2.x + a2.y;
         if (n & 1) a = fmaf(unpack2(g.P).x, win.read(p, n - 1), a);
-        acc.add(L.pref[b] * a);
       } else if constexpr (MODE == STRIP_MODE_CPU) {
-        float E = L.E0[b], R = L.R0[b];
+        float K = L.K0[b], R = L.R0[b];
 #pragma unroll 4
         for (int j = 0; j < n; ++j) {
-          a = fmaf(E, win.read(p, j), a);
-          E *= R;
+          a = fmaf(K, win.read(p, j), a);
+          K *= R;
           R *= k.q;
         }
-        acc.add(L.pref[b] * a);
       } else {
         AnalyticRow g;
         g.n0 = L.n0[b];
@@ -386,8 +371,8 @@ __device__ __forceinline__ void pass1_rows(const ScannerF& s, const KernelF& k,
 #pragma unroll 2
         for (int j = 0; j < n; ++j)
           a = fmaf(g.eval_t(k, fmaf((float)j, s.pw, L.t0[b])), win.read(p, j), a);
-        acc.add(a);
       }
+      acc.add(a);
     }
   }
 }
@@ -400,21 +385,23 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
                                            int lane, const LaneRows<MODE>& L,
                                            int nb, const Win& win,
                                            float scale) {
+  // the event's factor in the window's units (clamped: a denominator so
+  // small that 1 / D overflows still scatters finite values)
+  const float sc = WEIGHTED ? fminf(scale * win.unit(), 3.0e38f)
+                            : scale * win.unit();
 #pragma unroll
   for (int b = 0; b < kRowBlocks; ++b) {
-    const int n = run_len(L.lolen[b]);
+    const int n = run_len(L.run[b]);
     if (b < nb && n > 0) {
-      const auto p = win.ptr(e.tly + ranked_row(H, rank0 + 32 * b + lane),
-                             run_lo(L.lolen[b]));
+      const auto p = win.run_ptr(L.run[b], e, H, rank0 + 32 * b + lane);
       if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED && kPairs &&
-                    Win::pair_scatter() && Win::kShared) {
+                    Win::pair_scatter()) {
         // pass 1's walk (the same K values to the bit), u = K w / D in fixed
         // point with native shared integer reductions
-        const float E0 = L.E0[b], R0 = L.R0[b], R2 = R0 * R0;
-        float2 P = make_float2(E0, E0 * R0);
+        const float K0 = L.K0[b], R0 = L.R0[b], R2 = R0 * R0;
+        float2 P = make_float2(K0, K0 * R0);
         float2 S = make_float2(R2 * k.q, R2 * k.q3);
         const float2 Q4 = make_float2(k.q4, k.q4);
-        const float sc = fminf(L.pref[b] * scale * win.unit(), 3.0e38f);
         const float2 SC = make_float2(sc, sc);
         uint32_t ad = win.w_addr(p), aa = win.acc_addr(p);
 #pragma unroll 2
@@ -439,41 +426,38 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
           const float kw = P.x * lds32(ad);
           red_shared_add(aa, Win::fine() ? __float2uint_rn(kw * sc) : to_fixed(kw, sc));
         }
-      } else if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED && kPairs &&
-                    Win::pair_scatter()) {
-        PairRecurrence g(k, L.E0[b], L.R0[b]);
-        const float sc = fminf(L.pref[b] * scale * win.unit(), 3.0e38f);
-#pragma unroll 2
-        for (int j = 0; j + 1 < n; j += 2) {
-          win.add_weighted2(p, j, g.P, sc);
-          g.step();
-        }
-        if (n & 1) win.add_weighted(p, n - 1, unpack2(g.P).x, sc);
       } else if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED) {
-        float E = L.E0[b], R = L.R0[b];
-        const float sc = fminf(L.pref[b] * scale * win.unit(), 3.0e38f);
+        float K = L.K0[b], R = L.R0[b];
 #pragma unroll 4
         for (int j = 0; j < n; ++j) {
-          win.add_weighted(p, j, E, sc);
-          E *= R;
+          win.add_weighted(p, j, K, sc);
+          K *= R;
           R *= k.q;
         }
       } else if constexpr (MODE == STRIP_MODE_CPU && kPairs && Win::pair_add()) {
-        PairRecurrence g(k, L.E0[b], L.R0[b]);
-        const float sc = L.pref[b] * scale * win.unit();
+        // the adjoint's signed fixed point: K_j w_e, two pixels a step
+        const float K0 = L.K0[b], R0 = L.R0[b], R2 = R0 * R0;
+        float2 P = make_float2(K0, K0 * R0);
+        float2 S = make_float2(R2 * k.q, R2 * k.q3);
+        const float2 Q4 = make_float2(k.q4, k.q4);
+        const float2 SC = make_float2(sc, sc);
+        const float2 M = make_float2(kMagicSigned, kMagicSigned);
+        uint32_t aa = win.acc_addr(p);
 #pragma unroll 2
-        for (int j = 0; j + 1 < n; j += 2) {
-          win.add2(p, j, g.P, sc);
-          g.step();
+        for (int c = n >> 1; c > 0; --c, aa += 8) {
+          const float2 x = __ffma2_rn(P, SC, M);
+          red_shared_add(aa, __float_as_uint(x.x) - kMagicSignedBits);
+          red_shared_add(aa + 4, __float_as_uint(x.y) - kMagicSignedBits);
+          P = __fmul2_rn(P, S);
+          S = __fmul2_rn(S, Q4);
         }
-        if (n & 1) win.add(p, n - 1, unpack2(g.P).x * sc);
+        if (n & 1) win.add(p, n - 1, P.x * sc);
       } else if constexpr (MODE == STRIP_MODE_CPU) {
-        float E = L.E0[b], R = L.R0[b];
-        const float sc = L.pref[b] * scale * win.unit();
+        float K = L.K0[b], R = L.R0[b];
 #pragma unroll 4
         for (int j = 0; j < n; ++j) {
-          win.add(p, j, E * sc);
-          E *= R;
+          win.add(p, j, K * sc);
+          K *= R;
           R *= k.q;
         }
       } else {
@@ -485,7 +469,7 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
         g.cr = L.cr[b];
 #pragma unroll 2
         for (int j = 0; j < n; ++j)
-          win.add(p, j, g.eval_t(k, fmaf((float)j, s.pw, L.t0[b])) * scale);
+          win.add(p, j, g.eval_t(k, fmaf((float)j, s.pw, L.t0[b])) * sc);
       }
     }
   }
@@ -574,13 +558,15 @@ __device__ __forceinline__ void process_event(const LaunchArgs& a,
     grad_event(a, e, er, H, win, lane, aux.w);
     return;
   }
+  GaussEvent ge{};
+  if constexpr (MODE == STRIP_MODE_CPU) ge.init(a.k, a.s.R, e.tan, e.sec);
   constexpr int kSuper = 32 * kRowBlocks;
   LaneRows<MODE> L;
   float scale;
   if (OP == OP_MLEM || OP == OP_FORWARD) {
     RowSum<ACC> acc;
     for (int r0 = 0; r0 < H; r0 += kSuper) {
-      build_lane_rows<MODE>(a.s, a.k, e, er, H, r0, lane, L);
+      build_lane_rows<MODE>(a.s, a.k, e, er, ge, H, r0, lane, win, L);
       pass1_rows<MODE, ACC>(a.s, a.k, e, H, r0, lane, L,
                             min(kRowBlocks, (H - r0 + 31) >> 5), win, acc);
     }
@@ -603,7 +589,7 @@ __device__ __forceinline__ void process_event(const LaunchArgs& a,
     return;
   }
   for (int r0 = 0; r0 < H; r0 += kSuper) {
-    build_lane_rows<MODE>(a.s, a.k, e, er, H, r0, lane, L);
+    build_lane_rows<MODE>(a.s, a.k, e, er, ge, H, r0, lane, win, L);
     pass2_rows<MODE, kWeighted>(a.s, a.k, e, H, r0, lane, L,
                                 min(kRowBlocks, (H - r0 + 31) >> 5), win, scale);
   }

@@ -11,7 +11,7 @@
 // reference's A, B, C: dz = dy tan +- sqrt((9 - 4 sec^2 dy^2 / s_dl^2) s_z^2 / 2))
 // and its two ends are settled with the *exact* binary32 predicate
 // (strip_device.cuh), so the pixel set is the reference's bit for bit while
-// only ~4 pixels per row are tested instead of the whole row.
+// only 2 pixels per row are tested instead of the whole row.
 //
 // One warp handles one event.  build_rows() gives each lane one row of a
 // 32-row block, computes the row's exact run [lo, lo + len), its kernel row
@@ -82,9 +82,13 @@ __device__ __forceinline__ float sqrt_approx(float x) {
 // Rows whose closed-form run is at least kWideRun pixels wide: the closed
 // form locates each end within ~1e-4 px (binary32 rounding of q is <= ~1e-4
 // even for the most tilted ellipses here, k = |B| / (2 sqrt(A C)) <= 0.93,
-// while q changes by >= 2 C hw pw^2 >= 0.03 per pixel), so each end is one of
-// two adjacent columns and two exact tests per end settle it -- no loop, no
-// divergence.  Narrower rows (the ellipse's tips) take the general search.
+// while q changes by >= 2 C hw pw^2 >= 0.03 per pixel).  So with m the
+// column nearest to the closed-form end xl, every column left of m is at
+// least half a pixel outside (q > 9 + 0.015) and every column right of m up
+// to the centre at least half a pixel inside: the exact test of m alone
+// decides the end (lo = m or m + 1), and likewise at xh -- two exact tests
+// per row, no loop, no divergence.  Narrower rows (the ellipse's tips) take
+// the general search.
 constexpr float kWideRun = 1.0f;
 
 // Exact run of row iy within the box columns [tlx, brx): returns len, sets lo.
@@ -98,13 +102,9 @@ __device__ __forceinline__ int row_run(const ScannerF& s, const EventF& e,
   float xl = xv - hw, xh = xv + hw;
   int lo, hi;
   if (hw >= kWideRun && fabsf(xv) < 1e7f) {
-    const int lc = (int)ceilf(xl), hc = (int)floorf(xh);
-    const bool a = in_ellipse(rs, e.C, col_dz(s, e, lc - 1));
-    const bool b = in_ellipse(rs, e.C, col_dz(s, e, lc));
-    const bool c = in_ellipse(rs, e.C, col_dz(s, e, hc));
-    const bool d = in_ellipse(rs, e.C, col_dz(s, e, hc + 1));
-    lo = a ? lc - 1 : (b ? lc : lc + 1);
-    hi = d ? hc + 1 : (c ? hc : hc - 1);
+    const int ml = __float2int_rn(xl), mh = __float2int_rn(xh);
+    lo = in_ellipse(rs, e.C, col_dz(s, e, ml)) ? ml : ml + 1;
+    hi = in_ellipse(rs, e.C, col_dz(s, e, mh)) ? mh : mh - 1;
     lo = max(lo, cmin);
     hi = min(hi, cmax);
     lo_out = lo;
