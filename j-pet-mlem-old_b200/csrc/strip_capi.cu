@@ -78,6 +78,12 @@ ScannerF make_scanner(const strip_geometry& g) {
                  (double)sqrtf((s.ipsz * s.ipsz) * s.ipsdl));
   s.inv_pw = 1.0f / s.pw;
   s.inv2z = 0.5f / s.ipsz;
+  // A column half a pixel or more beyond a run end has q - 9 >=
+  // C pw^2 (1/4 + hw) (C = 2 ipsz, hw the run's half width in pixels); the
+  // two-test run ends need that margin far above the rounding of q (a few
+  // 1e-5): 2e-3 here, which every row meets when sigma_z <= ~22 pixels.
+  const double cpw2 = 2.0 * (double)s.ipsz * (double)s.pw * (double)s.pw;
+  s.min_closed_hw = (float)std::max(0.0, 2e-3 / cpw2 - 0.25);
   return s;
 }
 

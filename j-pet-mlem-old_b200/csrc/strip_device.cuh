@@ -21,8 +21,9 @@ struct ScannerF {
   float ipsz, ipsdl, kc;
   int n_y, n_z;  // after narrowing to int16, as Scanner<float, short>
   // launch constants of the closed-form row runs (not part of the exact
-  // set arithmetic): 1 / pw and sigma_z^2 / 2
-  float inv_pw, inv2z;
+  // set arithmetic): 1 / pw, sigma_z^2 / 2, and the smallest closed-form
+  // half width (pixels) whose run ends two exact tests settle
+  float inv_pw, inv2z, min_closed_hw;
 };
 
 // One event after Response::calculate_tan_y_z (response.h:22-37) and

@@ -577,7 +577,7 @@ __device__ __forceinline__ void process_event(const LaunchArgs& a,
     }
     // reconstruction.h:290 -- an all-zero denominator contributes nothing
     if (!(D > 0.0)) return;
-    scale = (float)(1.0 / D);
+    scale = rcp_approx((float)D);  // within an ulp of 1 / D; 0 or inf at the range ends
   } else {
     scale = (float)aux.w;  // OP_ADJOINT
     if (scale == 0.0f) return;

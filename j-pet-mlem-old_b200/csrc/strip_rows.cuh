@@ -79,18 +79,18 @@ __device__ __forceinline__ float sqrt_approx(float x) {
   return y;
 }
 
-// Rows whose closed-form run is at least kWideRun pixels wide: the closed
-// form locates each end within ~1e-4 px (binary32 rounding of q is <= ~1e-4
-// even for the most tilted ellipses here, k = |B| / (2 sqrt(A C)) <= 0.93,
-// while q changes by >= 2 C hw pw^2 >= 0.03 per pixel).  So with m the
-// column nearest to the closed-form end xl, every column left of m is at
-// least half a pixel outside (q > 9 + 0.015) and every column right of m up
-// to the centre at least half a pixel inside: the exact test of m alone
-// decides the end (lo = m or m + 1), and likewise at xh -- two exact tests
-// per row, no loop, no divergence.  Narrower rows (the ellipse's tips) take
-// the general search.
-constexpr float kWideRun = 1.0f;
-
+// Rows whose closed form is usable: the closed form locates each run end
+// within ~1e-4 px (binary32 rounding of q is <= ~1e-4 even for the most
+// tilted ellipses here, k = |B| / (2 sqrt(A C)) <= 0.93).  A column d >= 1/2
+// pixel beyond an end has q - 9 = C pw^2 (d^2 + 2 d hw) >= C pw^2 (1/4 + hw)
+// (hw the half width in pixels), far above that rounding whenever
+// hw >= s.min_closed_hw (0 for sigma_z <= ~22 pixels: every row, the
+// ellipse's tips and the empty rows of the box included).  So with m the
+// column nearest to the closed-form end xl, every column left of m is
+// outside and every column right of m up to the centre inside: the exact
+// test of m alone decides the end (lo = m or m + 1), and likewise at xh --
+// two exact tests per row, no loop, no divergence.  Other rows take the
+// general search.
 // Exact run of row iy within the box columns [tlx, brx): returns len, sets lo.
 __device__ __forceinline__ int row_run(const ScannerF& s, const EventF& e,
                                        const EventRows& er, const RowSet& rs,
@@ -101,7 +101,7 @@ __device__ __forceinline__ int row_run(const ScannerF& s, const EventF& e,
   const float xv = fmaf(e.tan * rs.dy, er.inv_pw, er.x0);
   float xl = xv - hw, xh = xv + hw;
   int lo, hi;
-  if (hw >= kWideRun && fabsf(xv) < 1e7f) {
+  if (hw >= s.min_closed_hw && fabsf(xv) < 1e7f) {
     const int ml = __float2int_rn(xl), mh = __float2int_rn(xh);
     lo = in_ellipse(rs, e.C, col_dz(s, e, ml)) ? ml : ml + 1;
     hi = in_ellipse(rs, e.C, col_dz(s, e, mh)) ? mh : mh - 1;
