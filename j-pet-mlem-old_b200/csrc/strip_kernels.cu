@@ -396,24 +396,24 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
       const auto p = win.run_ptr(L.run[b], e, H, rank0 + 32 * b + lane);
       if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED && kPairs &&
                     Win::pair_scatter()) {
-        // pass 1's walk (the same K values to the bit), u = K w / D in fixed
-        // point with native shared integer reductions
-        const float K0 = L.K0[b], R0 = L.R0[b], R2 = R0 * R0;
+        // pass 1's walk with K scaled by sc = unit / D from the start, so
+        // u = K w / D in fixed point is one FFMA per pixel (the 2^23 addend)
+        // and native shared integer reductions
+        const float K0 = L.K0[b] * sc, R0 = L.R0[b], R2 = R0 * R0;
         float2 P = make_float2(K0, K0 * R0);
         float2 S = make_float2(R2 * k.q, R2 * k.q3);
         const float2 Q4 = make_float2(k.q4, k.q4);
-        const float2 SC = make_float2(sc, sc);
         uint32_t ad = win.w_addr(p), aa = win.acc_addr(p);
 #pragma unroll 2
         for (int c = n >> 1; c > 0; --c, ad += 8, aa += 8) {
-          const float2 kw = __fmul2_rn(P, make_float2(lds32(ad), lds32(ad + 4)));
+          const float2 w2 = make_float2(lds32(ad), lds32(ad + 4));
           unsigned v0, v1;
           if constexpr (Win::fine()) {
-            const float2 x = __fmul2_rn(kw, SC);
+            const float2 x = __fmul2_rn(P, w2);
             v0 = __float2uint_rn(x.x);
             v1 = __float2uint_rn(x.y);
           } else {
-            const float2 x = __ffma2_rn(kw, SC, make_float2(kMagic, kMagic));
+            const float2 x = __ffma2_rn(P, w2, make_float2(kMagic, kMagic));
             v0 = __float_as_uint(x.x) - kMagicBits;
             v1 = __float_as_uint(x.y) - kMagicBits;
           }
@@ -423,8 +423,8 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
           S = __fmul2_rn(S, Q4);
         }
         if (n & 1) {
-          const float kw = P.x * lds32(ad);
-          red_shared_add(aa, Win::fine() ? __float2uint_rn(kw * sc) : to_fixed(kw, sc));
+          const float w = lds32(ad);
+          red_shared_add(aa, Win::fine() ? __float2uint_rn(P.x * w) : to_fixed(P.x, w));
         }
       } else if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED) {
         float K = L.K0[b], R = L.R0[b];
