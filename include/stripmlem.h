@@ -100,6 +100,9 @@ typedef struct strip_stats {
   double last_setup_ms;      /* device time of the last set_events binning     */
   double last_tile_ms;       /* device time of the tile-kernel launches of the
                                 last strip_iterate (CUDA events on the stream) */
+  int64_t n_fallback;        /* events of the last strip_iterate / accumulate
+                                that a tile's unweighted fixed-point window had
+                                no room for (rerun in a weighted window)       */
 } strip_stats;
 
 /* ---- context ------------------------------------------------------------ */

@@ -27,7 +27,7 @@
 using namespace stripmlem;
 
 // Windows up to this size let two CTAs share an SM.
-constexpr int kNarrowSmem = 113 * 1024;
+constexpr int kNarrowSmem = kNarrowSmemBytes;
 
 struct strip_batch {
   int device = 0;
@@ -159,7 +159,7 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
     b->n_events += c->n_events;
     for (int i = 0; i < b->args->member[m].n_items; ++i) {
       const WorkItem& w = c->items[i];
-      items.push_back(BatchItem{m, w.tile, w.count, cls, w.begin});
+      items.push_back(BatchItem{m, w.tile, w.count, cls, w.begin, i, 0});
     }
     b->launches_per_step += b->args->member[m].g_count > 0;
   }

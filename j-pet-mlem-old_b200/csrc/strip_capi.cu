@@ -127,7 +127,9 @@ int set_device(strip_ctx* ctx) {
 Tiling choose_tiling(const strip_ctx* ctx, int max_w, int max_h) {
   const int n_z = ctx->s.n_z, n_y = ctx->s.n_y;
   const int wide_budget = ctx->smem_optin - 2048;  // static shared memory
-  int budget = std::min(ctx->smem_optin, 113 * 1024);
+  // two CTAs per SM: 2 x (dynamic + ~1.1 KB static + 1 KB reserved) within
+  // the SM's 228 KB
+  int budget = std::min(ctx->smem_optin, kNarrowSmemBytes);
   Tiling t{};
   int TX = ctx->tile_pref, TY = ctx->tile_pref;
   int HX = max_w / 2 + 2, HY = max_h / 2 + 2;
@@ -280,12 +282,24 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
   }
   WorkItem* d_items = nullptr;
   CKB(cudaMalloc(&d_items, std::max<size_t>(items.size(), 1) * sizeof(WorkItem)));
+  float* d_ihist = nullptr;
+  {
+    const size_t hb = std::max<size_t>(items.size(), 1) * sizeof(float);
+    cudaError_t e = cudaMalloc(&d_ihist, hb);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_ihist, 0, hb, st);
+    if (e != cudaSuccess) {
+      cudaFree(d_items);
+      cudaFree(d_ihist);
+      CKB(e);
+    }
+  }
   if (!items.empty()) {
     cudaError_t e = cudaMemcpyAsync(d_items, items.data(),
                                     items.size() * sizeof(WorkItem),
                                     cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) {
       cudaFree(d_items);
+      cudaFree(d_ihist);
       CKB(e);
     }
   }
@@ -294,6 +308,7 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
       cudaFree(d_items);
+      cudaFree(d_ihist);
       CKB(e);
     }
   }
@@ -306,6 +321,8 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
   dfree(ctx->d_dl);
   dfree(ctx->d_perm);
   dfree(ctx->d_items);
+  dfree(ctx->d_item_hist);
+  ctx->d_item_hist = d_ihist;
   ctx->d_zu = ozu;
   ctx->d_zd = ozd;
   ctx->d_dl = odl;
@@ -374,7 +391,22 @@ LaunchArgs base_args(strip_ctx* ctx) {
   a.acc = ctx->d_acc;
   a.status = ctx->d_status;
   a.grab = ctx->grab;
+  // GaussianKernel values are at most kc / sqrt(2 R^2 ipsz): E <= 1 and
+  // a'Sa >= ipsz (ap^2 + aq^2) >= 2 R^2 ipsz sec^4
+  a.kbound = (float)((double)a.k.kc /
+                     ((double)ctx->s.R * std::sqrt(2.0 * (double)a.k.ipsz)) * 1.02);
+  a.n_fallback = ctx->d_fallback;
   return a;
+}
+
+// The work items and global-path range of OSEM subset sb, with the items'
+// unweighted-window statistics (MLEM).
+void set_subset(strip_ctx* ctx, LaunchArgs& a, int sb) {
+  a.items = ctx->d_items + ctx->sub_item_begin[sb];
+  a.item_hist = ctx->d_item_hist ? ctx->d_item_hist + ctx->sub_item_begin[sb] : nullptr;
+  a.n_items = ctx->sub_item_count[sb];
+  a.g_begin = ctx->sub_g_begin[sb];
+  a.g_count = ctx->sub_g_count[sb];
 }
 
 // Re-bins the resident events for n_subsets OSEM subsets when the current
@@ -452,12 +484,20 @@ int strip_ctx_create(const strip_geometry* g, int device, strip_ctx** out) {
     if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
     if (cudaMalloc(&ctx->d_rho, ctx->n_pix * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&ctx->d_acc_own, ctx->n_pix * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&ctx->d_status, sizeof(int)) != cudaSuccess) { rc = STRIP_E_NOMEM; break; }
+        cudaMalloc(&ctx->d_status, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_fallback, sizeof(unsigned long long)) != cudaSuccess) {
+      rc = STRIP_E_NOMEM;
+      break;
+    }
     ctx->d_acc = ctx->d_acc_own;
     std::vector<float> ones((size_t)ctx->n_pix, 1.0f);  // reconstruction.h:59
     if (cudaMemcpy(ctx->d_rho, ones.data(), ctx->n_pix * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(ctx->d_acc, 0, ctx->n_pix * sizeof(double)) != cudaSuccess ||
-        cudaMemset(ctx->d_status, 0, sizeof(int)) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
+        cudaMemset(ctx->d_status, 0, sizeof(int)) != cudaSuccess ||
+        cudaMemset(ctx->d_fallback, 0, sizeof(unsigned long long)) != cudaSuccess) {
+      rc = STRIP_E_CUDA;
+      break;
+    }
   } while (0);
   if (rc != STRIP_OK) {
     cudaGetLastError();
@@ -481,6 +521,8 @@ int strip_ctx_destroy(strip_ctx* ctx) {
   dfree(ctx->d_dl);
   dfree(ctx->d_perm);
   dfree(ctx->d_items);
+  dfree(ctx->d_item_hist);
+  dfree(ctx->d_fallback);
   dfree(ctx->d_status);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -582,6 +624,10 @@ int strip_set_image(strip_ctx* ctx, const float* rho) {
   if (int rc = set_device(ctx)) return rc;
   CK(cudaMemcpyAsync(ctx->d_rho, rho, ctx->n_pix * sizeof(float),
                      cudaMemcpyHostToDevice, ctx->stream));
+  // a new image: the next pass over each item starts from a weighted window
+  if (ctx->d_item_hist && !ctx->items.empty())
+    CK(cudaMemsetAsync(ctx->d_item_hist, 0, ctx->items.size() * sizeof(float),
+                       ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return STRIP_OK;
 }
@@ -631,6 +677,7 @@ int strip_iterate(strip_ctx* ctx, int n_iter, int mode, int n_subsets,
     ctx->tile_marks.push_back(ev);
   }
   size_t mark = 0;
+  CK(cudaMemsetAsync(ctx->d_fallback, 0, sizeof(unsigned long long), ctx->stream));
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   for (int it = 0; it < n_iter; ++it) {
     if (progress) {
@@ -638,10 +685,7 @@ int strip_iterate(strip_ctx* ctx, int n_iter, int mode, int n_subsets,
       progress(first + it, 0, user);
     }
     for (int sb = 0; sb < ctx->n_subsets; ++sb) {
-      a.items = ctx->d_items + ctx->sub_item_begin[sb];
-      a.n_items = ctx->sub_item_count[sb];
-      a.g_begin = ctx->sub_g_begin[sb];
-      a.g_count = ctx->sub_g_count[sb];
+      set_subset(ctx, a, sb);
       CK(cudaEventRecord(ctx->tile_marks[2 * mark], ctx->stream));
       CK(launch_tile(OP_MLEM, mode, ctx->accum, a, ctx->stream));
       CK(cudaEventRecord(ctx->tile_marks[2 * mark + 1], ctx->stream));
@@ -660,7 +704,11 @@ int strip_iterate(strip_ctx* ctx, int n_iter, int mode, int n_subsets,
     }
   }
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  unsigned long long n_fb = 0;
+  CK(cudaMemcpyAsync(&n_fb, ctx->d_fallback, sizeof(n_fb), cudaMemcpyDeviceToHost,
+                     ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  ctx->stats.n_fallback = (int64_t)n_fb;
   float ms = 0;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
   double tile_ms = 0;
@@ -706,10 +754,8 @@ int strip_accumulate(strip_ctx* ctx, int mode, int n_subsets, int subset) {
     if (int rc = ensure_sens5(ctx)) return rc;
   LaunchArgs a = base_args(ctx);
   a.sens = (mode == STRIP_MODE_GPU) ? ctx->d_sens5 : nullptr;
-  a.items = ctx->d_items + ctx->sub_item_begin[subset];
-  a.n_items = ctx->sub_item_count[subset];
-  a.g_begin = ctx->sub_g_begin[subset];
-  a.g_count = ctx->sub_g_count[subset];
+  set_subset(ctx, a, subset);
+  CK(cudaMemsetAsync(ctx->d_fallback, 0, sizeof(unsigned long long), ctx->stream));
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   CK(launch_tile(OP_MLEM, mode, ctx->accum, a, ctx->stream));
   CK(launch_global(OP_MLEM, mode, ctx->accum, a, ctx->stream));
@@ -1023,10 +1069,12 @@ int ctx_prepare_mlem(strip_ctx* ctx, int mode) {
 LaunchArgs ctx_mlem_args(strip_ctx* ctx, int mode) {
   LaunchArgs a = base_args(ctx);
   a.sens = (mode == STRIP_MODE_GPU) ? ctx->d_sens5 : nullptr;
-  a.items = ctx->d_items;
-  a.n_items = ctx->sub_item_count.empty() ? 0 : ctx->sub_item_count[0];
-  a.g_begin = ctx->sub_g_begin.empty() ? 0 : ctx->sub_g_begin[0];
-  a.g_count = ctx->sub_g_count.empty() ? 0 : ctx->sub_g_count[0];
+  if (ctx->sub_item_count.empty()) {
+    a.items = ctx->d_items;
+    a.n_items = 0;
+  } else {
+    set_subset(ctx, a, 0);
+  }
   return a;
 }
 

@@ -44,6 +44,10 @@ struct strip_ctx {
   std::vector<int> sub_item_begin, sub_item_count;
   std::vector<int64_t> sub_g_begin, sub_g_count;
   int* d_status = nullptr;
+  // per work item: the unweighted window statistic of the last pass (see
+  // LaunchArgs::item_hist); zeroed by a new binning and by strip_set_image
+  float* d_item_hist = nullptr;
+  unsigned long long* d_fallback = nullptr;  // events rerun in a weighted window
   std::vector<cudaEvent_t> tile_marks;
   strip_stats stats{};
   std::string err;

@@ -29,7 +29,22 @@ struct WorkItem {
 // largest s <= kMaxFixedShift for which (count + count/128 + 1) * 2^s <=
 // 2^32, so no pixel sum can wrap: s = 19 for the largest items
 // (kMaxItemEvents), 22 for 1016 events, 30 for the smallest.
+//
+// From the second pass over an item on, the window instead accumulates
+// K_j / D_e ("unweighted"): rho_j multiplies the pixel's sum once, when the
+// window is flushed, so the scatter walk reads no image values.  K_j / D_e
+// has no a-priori bound, so the scale comes from the item's previous pass:
+// with B the item's sum of 1 / D_e (kept as B times the window's mean image
+// value, so a rescaled image rescales it) the scale is the largest 2^s <=
+// 2^30 / (kbound B).  Before its scatter each event reserves its largest
+// addend, kbound 2^s / D_e, from a per-item budget of 2^32 - 2^24 (rounding
+// included), so no pixel sum can wrap.  An event that does not fit is not
+// scattered; once the unweighted window is flushed, those events run again
+// in a weighted window of their own.
 constexpr int kMaxFixedShift = 30;
+// Dynamic shared memory of a tile window that still runs two CTAs per SM.
+constexpr int kNarrowSmemBytes = 111 * 1024;
+constexpr float kFixedBudget = 4278190080.0f;  // 2^32 - 2^24
 constexpr int kMaxItemEvents = 8000;
 
 __host__ __device__ inline int fixed_shift(int count) {
@@ -92,9 +107,16 @@ struct LaunchArgs {
                          // OP_GRAD: in the caller's order
   double* grad_out;      // OP_GRAD: 2 doubles (atomic)
   double sz, sdl;        // OP_GRAD: model sigmas
-  float kbound;          // OP_ADJOINT: bound of the GaussianKernel values
+  float kbound;          // bound of the GaussianKernel values (OP_ADJOINT,
+                         // OP_MLEM with the reference CPU semantics)
   int grab;              // events a warp takes per counter step (1..32)
   int* status;           // device status word (0 = ok)
+  // OP_MLEM, GaussianKernel: per work item (indexed like `items`), the
+  // item's sum of 1 / D_e times its window's mean image value from the last
+  // pass over the item (0: none yet), which sizes the unweighted fixed-point
+  // window of the next pass; may be null
+  float* item_hist;
+  unsigned long long* n_fallback;  // events rerun in a weighted window, or null
 };
 
 // Several reconstructions in one persistent launch (strip_batch.cu): the
@@ -110,6 +132,8 @@ struct BatchItem {
   int32_t count;
   int32_t pad;    // host-side: the item's shared-memory class
   int64_t begin;
+  int32_t index;  // the item's index among its member's work items
+  int32_t pad2;
 };
 struct BatchUpdateArgs {
   int n;

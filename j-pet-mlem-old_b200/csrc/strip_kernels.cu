@@ -123,9 +123,20 @@ __device__ __forceinline__ int ranked_row(int H, int i) {
 //   kAccU32     unsigned fixed point, the 2^23 addend (rho-weighted MLEM)
 //   kAccU32Cvt  unsigned fixed point, cvt.rni (scales above 2^22)
 //   kAccS32     signed fixed point, the 1.5 * 2^23 addend (adjoint)
+//   kAccU32Unw  unsigned fixed point of K / D (cvt.rni), rho applied at the
+//               flush (MLEM from an item's second pass on)
 // The fixed-point kinds use native 32-bit integer shared atomics; the scale
 // `fixed_unit` is a power of two chosen per work item so that no sum wraps.
-enum AccKind { kAccF32 = 0, kAccU32 = 1, kAccU32Cvt = 2, kAccS32 = 3 };
+enum AccKind { kAccF32 = 0, kAccU32 = 1, kAccU32Cvt = 2, kAccS32 = 3, kAccU32Unw = 4 };
+
+// Per-CTA state of the work item in flight: the unweighted window's
+// fixed-point budget (units of 2^8), the item's sum of 1 / D_e, and the
+// events the unweighted window had no room for (bit i: event begin + i).
+constexpr unsigned kBudgetUnits = (unsigned)(kFixedBudget / 256.0f);
+__shared__ unsigned s_fx_budget;
+__shared__ float s_item_rsum;
+__shared__ unsigned s_fb_bits[kMaxItemEvents / 32];
+__shared__ int s_fb_n;
 
 template <int KIND>
 struct SmemWin {
@@ -170,6 +181,7 @@ struct SmemWin {
   }
   // signed fixed point: the adjoint's pair walk adds two pixels a step
   __host__ __device__ static constexpr bool pair_add() { return KIND == kAccS32; }
+  __host__ __device__ static constexpr bool unweighted() { return KIND == kAccU32Unw; }
   __host__ __device__ static constexpr bool fine() { return KIND == kAccU32Cvt; }
   // the rho-weighted MLEM scatter takes two pixels a step
   __host__ __device__ static constexpr bool pair_scatter() {
@@ -209,6 +221,7 @@ struct GlobalWin {
   __device__ __forceinline__ uint32_t acc_addr(int64_t) const { return 0; }
   __host__ __device__ static constexpr bool pair_scatter() { return false; }
   __host__ __device__ static constexpr bool pair_add() { return false; }
+  __host__ __device__ static constexpr bool unweighted() { return false; }
   __device__ __forceinline__ void add_weighted(int64_t p, int j, float E,
                                                float sc) const {
     atomicAdd(acc + p + j, (double)(E * read(p, j) * sc));
@@ -394,7 +407,22 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
     const int n = run_len(L.run[b]);
     if (b < nb && n > 0) {
       const auto p = win.run_ptr(L.run[b], e, H, rank0 + 32 * b + lane);
-      if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED && kPairs &&
+      if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED && Win::unweighted()) {
+        // K / D in fixed point: no image reads, one conversion per pixel
+        const float K0 = L.K0[b] * sc, R0 = L.R0[b], R2 = R0 * R0;
+        float2 P = make_float2(K0, K0 * R0);
+        float2 S = make_float2(R2 * k.q, R2 * k.q3);
+        const float2 Q4 = make_float2(k.q4, k.q4);
+        uint32_t aa = win.acc_addr(p);
+#pragma unroll 2
+        for (int c = n >> 1; c > 0; --c, aa += 8) {
+          red_shared_add(aa, __float2uint_rn(P.x));
+          red_shared_add(aa + 4, __float2uint_rn(P.y));
+          P = __fmul2_rn(P, S);
+          S = __fmul2_rn(S, Q4);
+        }
+        if (n & 1) red_shared_add(aa, __float2uint_rn(P.x));
+      } else if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED && kPairs &&
                     Win::pair_scatter()) {
         // pass 1's walk with K scaled by sc = unit / D from the start, so
         // u = K w / D in fixed point is one FFMA per pixel (the 2^23 addend)
@@ -547,16 +575,20 @@ __device__ __forceinline__ void grad_event(const LaunchArgs& a,
   }
 }
 
+// One event on one warp.  Returns 1 / D_e for an MLEM event with a positive
+// denominator (the work item's statistic), 0 otherwise; -1 / D_e for an
+// event the unweighted window had no room for (not scattered: the caller
+// runs it again in a weighted window).
 template <int OP, int MODE, int ACC, class Win>
-__device__ __forceinline__ void process_event(const LaunchArgs& a,
-                                              const EventF& e, const Win& win,
-                                              int lane, const EventAux& aux) {
+__device__ __forceinline__ float process_event(const LaunchArgs& a,
+                                               const EventF& e, const Win& win,
+                                               int lane, const EventAux& aux) {
   const int H = e.bry - e.tly;
-  if (H <= 0 || e.brx <= e.tlx) return;
+  if (H <= 0 || e.brx <= e.tlx) return 0.0f;
   const EventRows er = event_rows(a.s, e);
   if constexpr (OP == OP_GRAD) {
     grad_event(a, e, er, H, win, lane, aux.w);
-    return;
+    return 0.0f;
   }
   GaussEvent ge{};
   if constexpr (MODE == STRIP_MODE_CPU) ge.init(a.k, a.s.R, e.tan, e.sec);
@@ -573,26 +605,40 @@ __device__ __forceinline__ void process_event(const LaunchArgs& a,
     const double D = warp_sum(acc.total());
     if (OP == OP_FORWARD) {
       if (lane == 0) a.y_out[aux.out] = D;
-      return;
+      return 0.0f;
     }
     // reconstruction.h:290 -- an all-zero denominator contributes nothing
-    if (!(D > 0.0)) return;
+    if (!(D > 0.0)) return 0.0f;
     scale = rcp_approx((float)D);  // within an ulp of 1 / D; 0 or inf at the range ends
   } else {
     scale = (float)aux.w;  // OP_ADJOINT
-    if (scale == 0.0f) return;
+    if (scale == 0.0f) return 0.0f;
+  }
+  if constexpr (Win::unweighted()) {
+    // reserve the event's largest addend, kbound * unit / D (rounded up, in
+    // units of 2^8), from the item's fixed-point budget
+    const float need = a.kbound * scale * win.unit();
+    int ok = 0;
+    if (lane == 0 && need < kFixedBudget) {
+      const unsigned nu = (unsigned)(need * (1.0f / 256.0f)) + 1u;
+      const unsigned old = atomicAdd(&s_fx_budget, nu);
+      ok = old + nu <= kBudgetUnits;
+      if (!ok) atomicSub(&s_fx_budget, nu);
+    }
+    if (!__shfl_sync(kFull, ok, 0)) return -scale;
   }
   constexpr bool kWeighted = OP == OP_MLEM && MODE == STRIP_MODE_CPU;
   if ((OP == OP_MLEM) && H <= kSuper) {
     pass2_rows<MODE, kWeighted>(a.s, a.k, e, H, 0, lane, L, (H + 31) >> 5, win,
                                 scale);
-    return;
+    return scale;
   }
   for (int r0 = 0; r0 < H; r0 += kSuper) {
     build_lane_rows<MODE>(a.s, a.k, e, er, ge, H, r0, lane, win, L);
     pass2_rows<MODE, kWeighted>(a.s, a.k, e, H, r0, lane, L,
                                 min(kRowBlocks, (H - r0 + 31) >> 5), win, scale);
   }
+  return OP == OP_MLEM ? scale : 0.0f;
 }
 
 __device__ __forceinline__ RowTables warp_tables(char* base, int cap, int warp) {
@@ -631,13 +677,17 @@ __device__ int adjoint_shift(const LaunchArgs& a, const WorkItem& it, int lane) 
 
 // The events of a work item: warps pull groups of a.grab (1..32) events from
 // a shared counter until the item is done (lanes < a.grab set the group's
-// events up in parallel).
+// events up in parallel).  With `only`, just the events whose bit is set:
+// the rerun, in a weighted window, of the events an unweighted window had no
+// room for (their 1 / D_e is counted already).
 template <int OP, int MODE, int ACC, class Win>
 __device__ __forceinline__ void run_item(const LaunchArgs& a, const WorkItem& it,
                                          const Win& win, int lane,
-                                         int* next_group) {
+                                         int* next_group,
+                                         const unsigned* only = nullptr) {
   const int64_t end = it.begin + it.count;
   const int grab = a.grab;
+  float rsum = 0.0f;  // this warp's sum of 1 / D_e
   for (;;) {
     int g = 0;
     if (lane == 0) g = atomicAdd(next_group, 1);
@@ -648,33 +698,74 @@ __device__ __forceinline__ void run_item(const LaunchArgs& a, const WorkItem& it
     EventF mine = {};
     EventAux aux;
     if (lane < grab && ei < end) {
-      aux = load_aux<OP>(a, ei);
-      event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], mine);
+      const int off = (int)(ei - it.begin);
+      if (!only || ((only[off >> 5] >> (off & 31)) & 1u)) {
+        aux = load_aux<OP>(a, ei);
+        event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], mine);
+      }
     }
     const int nh = (int)min((int64_t)grab, end - base);
     for (int j = 0; j < nh; ++j) {
       const EventF e = shfl_event(mine, j);
-      process_event<OP, MODE, ACC>(a, e, win, lane, shfl_aux<OP>(aux, j));
+      const float r = process_event<OP, MODE, ACC>(a, e, win, lane, shfl_aux<OP>(aux, j));
+      if (r < 0.0f) {  // not scattered: no room in the unweighted window
+        if (lane == 0) {
+          const int off = (int)(base + j - it.begin);
+          atomicOr(&s_fb_bits[off >> 5], 1u << (off & 31));
+          atomicAdd(&s_fb_n, 1);
+        }
+        rsum -= r;
+      } else {
+        rsum += r;
+      }
     }
   }
+  if (OP == OP_MLEM && lane == 0 && !only && rsum != 0.0f) atomicAdd(&s_item_rsum, rsum);
+}
+
+// Sum of v over the CTA, returned to every thread (two barriers).
+__device__ __forceinline__ float block_sum(float v) {
+  __shared__ float s_part[kWarps];
+  __shared__ float s_total;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.0f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_part[w];
+    s_total = t;
+  }
+  __syncthreads();
+  return s_total;
 }
 
 // One work item on the whole CTA: stage the window, run the events, flush.
-// The CTA may run further items afterwards (the batched kernel): the caller
-// synchronises before the shared memory is reused.
+// `index` is the item's index among the launch's items (its statistic in
+// a.item_hist).  The CTA may run further items afterwards (the batched
+// kernel): the caller synchronises before the shared memory is reused.
 template <int OP, int MODE, int ACC>
 __device__ __forceinline__ void tile_item(const LaunchArgs& a,
-                                          const WorkItem it, char* smem_raw,
-                                          int* s_next_group) {
+                                          const WorkItem it, int index,
+                                          char* smem_raw, int* s_next_group) {
   int wx0, wy0, wx1, wy1;
   tile_window(a.t, a.s.n_z, a.s.n_y, it.tile, wx0, wy0, wx1, wy1);
   const int wxn = wx1 - wx0, wyn = wy1 - wy0, WS = a.t.WS;
   float* s_w = reinterpret_cast<float*>(smem_raw);
   float* s_acc = s_w + a.t.WYmax * WS;
-  if (threadIdx.x == 0) *s_next_group = 0;
-  const int lane = threadIdx.x & 31;
   constexpr bool kReads = (OP != OP_ADJOINT);
   constexpr bool kWrites = (OP == OP_MLEM || OP == OP_ADJOINT);
+  constexpr bool kFixedMlem = (OP == OP_MLEM && MODE == STRIP_MODE_CPU);
+  if (threadIdx.x == 0) {
+    *s_next_group = 0;
+    s_fx_budget = 0u;
+    s_item_rsum = 0.0f;
+    s_fb_n = 0;
+  }
+  if (kFixedMlem)
+    for (int q = threadIdx.x; q < kMaxItemEvents / 32; q += blockDim.x) s_fb_bits[q] = 0u;
+  const int lane = threadIdx.x & 31;
+  float wsum = 0.0f;
   for (int q = threadIdx.x; q < wxn * wyn; q += blockDim.x) {
     const int r = q / wxn, c = q - r * wxn;
     const int64_t gi = (int64_t)(wy0 + r) * a.s.n_z + wx0 + c;
@@ -682,62 +773,109 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
       float v = a.rho[gi];
       if (MODE == STRIP_MODE_GPU) v *= a.sens[gi];
       s_w[r * WS + c] = v;
+      wsum += v;
     }
     if (kWrites) s_acc[r * WS + c] = 0.0f;
   }
   __syncthreads();
-  // fixed-point scale 2^fshift of the window accumulator
-  int fshift = 0;
-  if constexpr (OP == OP_MLEM && MODE == STRIP_MODE_CPU) {
-    fshift = fixed_shift(it.count);
-  } else if constexpr (OP == OP_ADJOINT && MODE == STRIP_MODE_CPU) {
-    fshift = adjoint_shift(a, it, lane);
-  }
-  const float unit = exp2f((float)fshift);
   const uint32_t w_sh = (uint32_t)__cvta_generic_to_shared(s_w);
   const uint32_t acc_sh = (uint32_t)__cvta_generic_to_shared(s_acc);
-  if constexpr (OP == OP_MLEM && MODE == STRIP_MODE_CPU) {
-    if (fshift > 22)
-      run_item<OP, MODE, ACC>(
-          a, it, SmemWin<kAccU32Cvt>{s_w, s_acc, wx0, wy0, WS, unit, w_sh, acc_sh}, lane,
-          s_next_group);
-    else
-      run_item<OP, MODE, ACC>(
-          a, it, SmemWin<kAccU32>{s_w, s_acc, wx0, wy0, WS, unit, w_sh, acc_sh}, lane,
-          s_next_group);
-  } else if constexpr (OP == OP_ADJOINT && MODE == STRIP_MODE_CPU) {
-    run_item<OP, MODE, ACC>(a, it,
-                            SmemWin<kAccS32>{s_w, s_acc, wx0, wy0, WS, unit, w_sh, acc_sh},
-                            lane, s_next_group);
-  } else {
-    run_item<OP, MODE, ACC>(a, it,
-                            SmemWin<kAccF32>{s_w, s_acc, wx0, wy0, WS, 1.0f, w_sh, acc_sh},
-                            lane, s_next_group);
-  }
-  if (kWrites) {
-    __syncthreads();
-    const unsigned* s_acc_u = reinterpret_cast<const unsigned*>(s_acc);
+  // Adds the window accumulator (fixed point at scale 2^fshift, times the
+  // image value for an unweighted window, which is zeroed on the way) into
+  // the global binary64 accumulator.
+  auto flush = [&](int fshift, bool unweighted) {
+    unsigned* s_acc_u = reinterpret_cast<unsigned*>(s_acc);
     const int* s_acc_i = reinterpret_cast<const int*>(s_acc);
     for (int q = threadIdx.x; q < wxn * wyn; q += blockDim.x) {
       const int r = q / wxn, c = q - r * wxn;
       double v;
-      if constexpr (OP == OP_MLEM && MODE == STRIP_MODE_CPU)
+      if constexpr (kFixedMlem) {
         v = ldexp((double)s_acc_u[r * WS + c], -fshift);
-      else if constexpr (OP == OP_ADJOINT && MODE == STRIP_MODE_CPU)
+        if (unweighted) {
+          v *= (double)s_w[r * WS + c];
+          s_acc_u[r * WS + c] = 0u;
+        }
+      } else if constexpr (OP == OP_ADJOINT && MODE == STRIP_MODE_CPU) {
         v = ldexp((double)s_acc_i[r * WS + c], -fshift);
-      else
+      } else {
         v = (double)s_acc[r * WS + c];
+      }
       if (v != 0.0)
         atomicAdd(a.acc + (int64_t)(wy0 + r) * a.s.n_z + wx0 + c, v);
+    }
+  };
+  // A weighted MLEM window over `count` events of the item (those of `only`,
+  // or all); returns its scale's exponent.
+  auto run_weighted = [&](int count, const unsigned* only) {
+    const int fs = fixed_shift(count);
+    run_item<OP, MODE, ACC>(
+        a, it, SmemWin<kAccU32Cvt>{s_w, s_acc, wx0, wy0, WS, exp2f((float)fs), w_sh, acc_sh},
+        lane, s_next_group, only);
+    return fs;
+  };
+  if constexpr (kFixedMlem) {
+    // the unweighted window once the item has a statistic, else weighted
+    const float wmean = block_sum(wsum) / (float)(wxn * wyn);
+    const float hist = a.item_hist ? a.item_hist[index] : 0.0f;
+    const float B = hist / wmean;  // this pass's sum of 1 / D_e, estimated
+    const float lim = 1073741824.0f / (a.kbound * B);  // 2^30 / (kbound B)
+    int fshift = 0;
+    bool unweighted = false;
+    if (hist > 0.0f && wmean > 0.0f && B > 0.0f && B < 3.0e38f && lim > 0.0f &&
+        lim < 3.0e38f) {
+      fshift = (int)floorf(log2f(lim));
+      unweighted = fshift >= -120 && fshift <= 120;
+    }
+    if (unweighted) {
+      run_item<OP, MODE, ACC>(
+          a, it,
+          SmemWin<kAccU32Unw>{s_w, s_acc, wx0, wy0, WS, exp2f((float)fshift), w_sh, acc_sh},
+          lane, s_next_group);
+      __syncthreads();
+      flush(fshift, true);
+      const int n_fb = s_fb_n;
+      if (n_fb > 0) {  // the events that found no room, in a weighted window
+        __syncthreads();  // the flush has zeroed the window accumulator
+        if (threadIdx.x == 0) {
+          *s_next_group = 0;
+          if (a.n_fallback) atomicAdd(a.n_fallback, (unsigned long long)n_fb);
+        }
+        __syncthreads();
+        const int fs = run_weighted(n_fb, s_fb_bits);
+        __syncthreads();
+        flush(fs, false);
+      }
+    } else {
+      const int fs = run_weighted(it.count, nullptr);
+      __syncthreads();
+      flush(fs, false);
+    }
+    if (threadIdx.x == 0 && a.item_hist) a.item_hist[index] = s_item_rsum * wmean;
+  } else if constexpr (OP == OP_ADJOINT && MODE == STRIP_MODE_CPU) {
+    const int fshift = adjoint_shift(a, it, lane);
+    run_item<OP, MODE, ACC>(
+        a, it,
+        SmemWin<kAccS32>{s_w, s_acc, wx0, wy0, WS, exp2f((float)fshift), w_sh, acc_sh},
+        lane, s_next_group);
+    __syncthreads();
+    flush(fshift, false);
+  } else {
+    run_item<OP, MODE, ACC>(a, it,
+                            SmemWin<kAccF32>{s_w, s_acc, wx0, wy0, WS, 1.0f, w_sh, acc_sh},
+                            lane, s_next_group);
+    if (kWrites) {
+      __syncthreads();
+      flush(0, false);
     }
   }
 }
 
 template <int OP, int MODE, int ACC>
-__global__ void __launch_bounds__(kThreads, 2) k_tile(LaunchArgs a) {  // 2 CTAs x 16 warps per SM
+__global__ void __launch_bounds__(kThreads, 2) k_tile(const __grid_constant__ LaunchArgs a) {  // 2 CTAs x 16 warps per SM
   extern __shared__ __align__(16) char smem_raw[];
   __shared__ int s_next_group;
-  tile_item<OP, MODE, ACC>(a, a.items[blockIdx.x], smem_raw, &s_next_group);
+  tile_item<OP, MODE, ACC>(a, a.items[blockIdx.x], blockIdx.x, smem_raw,
+                           &s_next_group);
 }
 
 // Persistent tile kernel over the work items of several reconstructions: a
@@ -758,7 +896,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const BatchItem bi = items[i];
     tile_item<OP_MLEM, MODE, ACC>(b.member[bi.member],
                                   WorkItem{bi.tile, bi.count, bi.begin},
-                                  smem_raw, &s_next_group);
+                                  bi.index, smem_raw, &s_next_group);
     __syncthreads();  // before the next item's window overwrites this one
   }
 }

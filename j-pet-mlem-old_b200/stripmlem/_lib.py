@@ -90,6 +90,7 @@ class Stats(ctypes.Structure):
         ("last_iterate_ms", ctypes.c_double),
         ("last_setup_ms", ctypes.c_double),
         ("last_tile_ms", ctypes.c_double),
+        ("n_fallback", ctypes.c_int64),
     ]
 
 
