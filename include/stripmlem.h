@@ -265,6 +265,14 @@ int strip_debug_pixel_sets(strip_ctx* ctx, const float* z_u, const float* z_d,
                            const float* dl, int64_t n, int32_t* n_bb,
                            int32_t* n_in, uint64_t* digest);
 
+/* Multiplies the per-work-item statistics that size the unweighted
+ * fixed-point windows of the next MLEM pass by `factor` (> 0).  A factor
+ * below 1 makes the next pass's windows too fine for their events, so events
+ * run out of room and take the weighted rerun (strip_stats.n_fallback): a
+ * test of that path.  Results stay correct for any factor; only the
+ * speed changes.  No counterpart in the reference. */
+int strip_debug_scale_item_stats(strip_ctx* ctx, float factor);
+
 /* ---- allocation-free iteration ----------------------------------------- */
 
 /* Largest image (n_y * n_z pixels) strip_iterate_noalloc accepts. */

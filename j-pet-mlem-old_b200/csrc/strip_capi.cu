@@ -1017,6 +1017,21 @@ int strip_probe_fp32_peak(int device, double* tflops) {
   return STRIP_OK;
 }
 
+int strip_debug_scale_item_stats(strip_ctx* ctx, float factor) {
+  if (!ctx || !(factor > 0.0f) || !std::isfinite(factor)) return STRIP_E_INVALID;
+  if (int rc = set_device(ctx)) return rc;
+  if (!ctx->d_item_hist || ctx->items.empty()) return STRIP_OK;
+  std::vector<float> h(ctx->items.size());
+  CK(cudaMemcpyAsync(h.data(), ctx->d_item_hist, h.size() * sizeof(float),
+                     cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (float& v : h) v *= factor;
+  CK(cudaMemcpyAsync(ctx->d_item_hist, h.data(), h.size() * sizeof(float),
+                     cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return STRIP_OK;
+}
+
 int strip_debug_pixel_sets(strip_ctx* ctx, const float* zu, const float* zd,
                            const float* dl, int64_t n, int32_t* n_bb,
                            int32_t* n_in, uint64_t* digest) {

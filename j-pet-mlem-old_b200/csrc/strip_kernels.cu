@@ -463,23 +463,22 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
           R *= k.q;
         }
       } else if constexpr (MODE == STRIP_MODE_CPU && kPairs && Win::pair_add()) {
-        // the adjoint's signed fixed point: K_j w_e, two pixels a step
-        const float K0 = L.K0[b], R0 = L.R0[b], R2 = R0 * R0;
+        // the adjoint's signed fixed point: K_j w_e with w_e and the unit
+        // folded into the run's first value, two pixels a step, one
+        // conversion per pixel
+        const float K0 = L.K0[b] * sc, R0 = L.R0[b], R2 = R0 * R0;
         float2 P = make_float2(K0, K0 * R0);
         float2 S = make_float2(R2 * k.q, R2 * k.q3);
         const float2 Q4 = make_float2(k.q4, k.q4);
-        const float2 SC = make_float2(sc, sc);
-        const float2 M = make_float2(kMagicSigned, kMagicSigned);
         uint32_t aa = win.acc_addr(p);
 #pragma unroll 2
         for (int c = n >> 1; c > 0; --c, aa += 8) {
-          const float2 x = __ffma2_rn(P, SC, M);
-          red_shared_add(aa, __float_as_uint(x.x) - kMagicSignedBits);
-          red_shared_add(aa + 4, __float_as_uint(x.y) - kMagicSignedBits);
+          red_shared_add(aa, (unsigned)__float2int_rn(P.x));
+          red_shared_add(aa + 4, (unsigned)__float2int_rn(P.y));
           P = __fmul2_rn(P, S);
           S = __fmul2_rn(S, Q4);
         }
-        if (n & 1) win.add(p, n - 1, P.x * sc);
+        if (n & 1) red_shared_add(aa, (unsigned)__float2int_rn(P.x));
       } else if constexpr (MODE == STRIP_MODE_CPU) {
         float K = L.K0[b], R = L.R0[b];
 #pragma unroll 4
@@ -752,7 +751,8 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
   tile_window(a.t, a.s.n_z, a.s.n_y, it.tile, wx0, wy0, wx1, wy1);
   const int wxn = wx1 - wx0, wyn = wy1 - wy0, WS = a.t.WS;
   float* s_w = reinterpret_cast<float*>(smem_raw);
-  float* s_acc = s_w + a.t.WYmax * WS;
+  // the adjoint reads no image: its accumulator is the only window
+  float* s_acc = OP == OP_ADJOINT ? s_w : s_w + a.t.WYmax * WS;
   constexpr bool kReads = (OP != OP_ADJOINT);
   constexpr bool kWrites = (OP == OP_MLEM || OP == OP_ADJOINT);
   constexpr bool kFixedMlem = (OP == OP_MLEM && MODE == STRIP_MODE_CPU);
@@ -870,8 +870,26 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
   }
 }
 
+// CTAs per SM a tile kernel is compiled for: MLEM keeps two windows (image
+// and accumulator) and up to 64 registers a thread (2 x 16 warps per SM);
+// the GaussianKernel forward and adjoint keep one window each and fit 40
+// registers, for 3 x 16 warps.
+#ifndef STRIP_ADJ_CTAS
+#define STRIP_ADJ_CTAS 3
+#endif
+template <int OP, int MODE>
+constexpr int tile_ctas_per_sm() {
+  return MODE != STRIP_MODE_CPU ? 2
+         : OP == OP_FORWARD    ? 3
+         : OP == OP_ADJOINT    ? STRIP_ADJ_CTAS
+                               : 2;
+}
+template <int OP>
+constexpr int tile_windows() { return OP == OP_MLEM ? 2 : 1; }
+
 template <int OP, int MODE, int ACC>
-__global__ void __launch_bounds__(kThreads, 2) k_tile(const __grid_constant__ LaunchArgs a) {  // 2 CTAs x 16 warps per SM
+__global__ void __launch_bounds__(kThreads, tile_ctas_per_sm<OP, MODE>())
+    k_tile(const __grid_constant__ LaunchArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   __shared__ int s_next_group;
   tile_item<OP, MODE, ACC>(a, a.items[blockIdx.x], blockIdx.x, smem_raw,
@@ -1181,10 +1199,11 @@ constexpr int kSetsCap = 64;
 template <int OP, int MODE, int ACC>
 cudaError_t launch_tile_t(const LaunchArgs& a, cudaStream_t st) {
   auto fn = k_tile<OP, MODE, ACC>;
+  const int smem = a.t.smem_bytes / 2 * tile_windows<OP>();
   cudaError_t err = cudaFuncSetAttribute(
-      fn, cudaFuncAttributeMaxDynamicSharedMemorySize, a.t.smem_bytes);
+      fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (err != cudaSuccess) return err;
-  fn<<<a.n_items, kThreads, a.t.smem_bytes, st>>>(a);
+  fn<<<a.n_items, kThreads, smem, st>>>(a);
   return cudaGetLastError();
 }
 

@@ -169,6 +169,7 @@ SIGNATURES = {
         ctypes.c_int,
         [_ctx, _f, _f, _f, ctypes.c_int64, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_uint64)],
     ),
+    "strip_debug_scale_item_stats": (ctypes.c_int, [_ctx, ctypes.c_float]),
     "strip_iterate_noalloc": (
         ctypes.c_int,
         [_P(Geometry), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
