@@ -120,11 +120,14 @@ __device__ __forceinline__ float col_dz(const ScannerF& s, const EventF& e,
   const float pz = __fadd_rn(s.tl_z_half_w, __fmul_rn((float)iz, s.pw));
   return __fsub_rn(pz, e.z);
 }
-// (A*dy*dy) + (B*dy*dz) + (C*dz*dz) <= 9, summed left to right.
+// (A*dy*dy) + (B*dy*dz) + (C*dz*dz), summed left to right; in the ellipse
+// when <= 9.
+__device__ __forceinline__ float row_q(const RowSet& r, float C, float dz) {
+  return __fadd_rn(__fadd_rn(r.Ady2, __fmul_rn(r.Bdy, dz)),
+                   __fmul_rn(__fmul_rn(C, dz), dz));
+}
 __device__ __forceinline__ bool in_ellipse(const RowSet& r, float C, float dz) {
-  const float q = __fadd_rn(__fadd_rn(r.Ady2, __fmul_rn(r.Bdy, dz)),
-                            __fmul_rn(__fmul_rn(C, dz), dz));
-  return q <= 9.0f;
+  return row_q(r, C, dz) <= 9.0f;
 }
 
 __device__ __forceinline__ uint64_t mix64(uint64_t x) {

@@ -287,8 +287,8 @@ struct LaneRows<STRIP_MODE_GPU> {
 };
 
 // Builds the lane's rows of ranks [rank0, rank0 + 32*kRowBlocks).
-template <int MODE, class Win>
-__device__ __forceinline__ void build_lane_rows(const ScannerF& s,
+template <int MODE, bool CLOSED_ONLY, class Win>
+__device__ __forceinline__ void build_lane_rows_t(const ScannerF& s,
                                                 const KernelF& k,
                                                 const EventF& e,
                                                 const EventRows& er,
@@ -304,7 +304,7 @@ __device__ __forceinline__ void build_lane_rows(const ScannerF& s,
       const int iy = e.tly + ranked_row(H, i);
       const RowSet rs = row_set(s, e, iy);
       int lo;
-      const int len = row_run(s, e, er, rs, lo);
+      const int len = row_run<CLOSED_ONLY>(s, e, er, rs, lo);
       L.run[b] = win.pack_run(iy, lo, len);
       if (len > 0) {
         const float t0 = (fmaf((float)lo, s.pw, s.tl_z_half_w) - e.z);
@@ -323,6 +323,23 @@ __device__ __forceinline__ void build_lane_rows(const ScannerF& s,
       }
     }
   }
+}
+
+// The same, with the row runs' general search compiled out when the
+// geometry lets the closed form settle every row (uniform per launch).
+template <int MODE, class Win>
+__device__ __forceinline__ void build_lane_rows(const ScannerF& s,
+                                                const KernelF& k,
+                                                const EventF& e,
+                                                const EventRows& er,
+                                                const GaussEvent& ge, int H,
+                                                int rank0, int lane,
+                                                const Win& win,
+                                                LaneRows<MODE>& L) {
+  if (s.min_closed_hw == 0.0f)
+    build_lane_rows_t<MODE, true>(s, k, e, er, ge, H, rank0, lane, win, L);
+  else
+    build_lane_rows_t<MODE, false>(s, k, e, er, ge, H, rank0, lane, win, L);
 }
 
 // Pass 1 over the lane's rows: sum over runs of K_j * w_j.
@@ -1128,7 +1145,9 @@ __global__ void __launch_bounds__(kThreads) k_sets(
       for (int r0 = 0; r0 < H; r0 += cap) {
         const int nr = min(cap, H - r0);
         if (r0 > 0) __syncwarp();
-        const int m = build_rows<0>(s, k, e, er, e.tly + r0, nr, T, lane);
+        const int m = s.min_closed_hw == 0.0f
+                          ? build_rows<0, true>(s, k, e, er, e.tly + r0, nr, T, lane)
+                          : build_rows<0, false>(s, k, e, er, e.tly + r0, nr, T, lane);
         cnt += m;
         if (DEBUG) {
           walk_share(T, nr, m, lane, [&](int r, int col, int c) {

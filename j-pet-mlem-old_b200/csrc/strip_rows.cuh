@@ -92,6 +92,11 @@ __device__ __forceinline__ float sqrt_approx(float x) {
 // two exact tests per row, no loop, no divergence.  Other rows take the
 // general search.
 // Exact run of row iy within the box columns [tlx, brx): returns len, sets lo.
+// CLOSED_ONLY: the geometry lets the closed form settle every row
+// (s.min_closed_hw == 0), so the general search is compiled out; a row whose
+// centre column is not finite or lies 1e7 columns away is empty (its ellipse
+// cannot reach the box), as the general search finds.
+template <bool CLOSED_ONLY = false>
 __device__ __forceinline__ int row_run(const ScannerF& s, const EventF& e,
                                        const EventRows& er, const RowSet& rs,
                                        int& lo_out) {
@@ -101,10 +106,16 @@ __device__ __forceinline__ int row_run(const ScannerF& s, const EventF& e,
   const float xv = fmaf(e.tan * rs.dy, er.inv_pw, er.x0);
   float xl = xv - hw, xh = xv + hw;
   int lo, hi;
-  if (hw >= s.min_closed_hw && fabsf(xv) < 1e7f) {
+  if (CLOSED_ONLY || (hw >= s.min_closed_hw && fabsf(xv) < 1e7f)) {
+    if (CLOSED_ONLY && !(fabsf(xv) < 1e7f)) {
+      lo_out = cmin;
+      return 0;
+    }
     const int ml = __float2int_rn(xl), mh = __float2int_rn(xh);
-    lo = in_ellipse(rs, e.C, col_dz(s, e, ml)) ? ml : ml + 1;
-    hi = in_ellipse(rs, e.C, col_dz(s, e, mh)) ? mh : mh - 1;
+    const float ql = row_q(rs, e.C, col_dz(s, e, ml));
+    const float qh = row_q(rs, e.C, col_dz(s, e, mh));
+    lo = ql <= 9.0f ? ml : ml + 1;
+    hi = qh <= 9.0f ? mh : mh - 1;
     lo = max(lo, cmin);
     hi = min(hi, cmax);
     lo_out = lo;
@@ -133,7 +144,7 @@ __device__ __forceinline__ int row_run(const ScannerF& s, const EventF& e,
 // KC: 0 = no kernel constants, 1 = GaussRow, 2 = AnalyticRow.  Returns the
 // number of pixels in those rows (same value in every lane).  Ends with a
 // __syncwarp(); the caller must __syncwarp() before rebuilding.
-template <int KC>
+template <int KC, bool CLOSED_ONLY = false>
 __device__ __forceinline__ int build_rows(const ScannerF& s, const KernelF& k,
                                           const EventF& e, const EventRows& er,
                                           int row0, int nrows,
@@ -146,7 +157,7 @@ __device__ __forceinline__ int build_rows(const ScannerF& s, const KernelF& k,
     if (r < nrows) {
       const RowSet rs = row_set(s, e, row0 + r);
       int lo;
-      len = row_run(s, e, er, rs, lo);
+      len = row_run<CLOSED_ONLY>(s, e, er, rs, lo);
       T.lo[r] = lo;
       if (KC == 1) {
         GaussRow g;
