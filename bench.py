@@ -47,8 +47,8 @@ PHANTOM = [
 SEED = 20260101
 # DRAM bytes (read + write) per event of one k_tile pass, from an ncu capture
 # of this workload's first 2e7 events (profiles/k_tile_strip_c2_2e7events.md:
-# 246.8 MB read + 5.0 MB written); the traffic grows with the event count.
-TILE_DRAM_BYTES_PER_EVENT = (246.809344e6 + 5.007360e6) / 2e7
+# 245.1 MB read + 5.4 MB written); the traffic grows with the event count.
+TILE_DRAM_BYTES_PER_EVENT = (245.074176e6 + 5.365504e6) / 2e7
 
 
 def workload_config(n_events, e2e_iters, world=1):
