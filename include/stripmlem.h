@@ -247,11 +247,11 @@ typedef struct strip_tuning {
 } strip_tuning;
 /* Times one MLEM backprojection of the context's events (into scratch: the
  * image and accumulator are untouched) for every schedule of tile edge
- * {16, 32, 48, 64} x grab {4, 8, 16}, keeps the fastest (events re-binned
+ * {16, 32, 48, 64} x grab {4, 8, 16, 32}, keeps the fastest (events re-binned
  * for it) and reports it in *best (may be NULL). */
 int strip_autotune(strip_ctx* ctx, int mode, strip_tuning* best);
 /* Sets the schedule by hand (tile edge 8..128, grab 1..32); re-bins the
- * events when the context has some.  Defaults: tile 32, grab 16. */
+ * events when the context has some.  Defaults: tile 32, grab 32. */
 int strip_set_schedule(strip_ctx* ctx, int tile, int grab);
 
 /* ---- parity ----------------------------------------------------------- */

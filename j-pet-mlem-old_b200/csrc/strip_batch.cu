@@ -265,7 +265,7 @@ int strip_autotune(strip_ctx* ctx, int mode, strip_tuning* best) {
     return STRIP_E_INVALID;
   if (int rc = ctx_prepare_mlem(ctx, mode)) return rc;
   static const int kTiles[] = {16, 32, 48, 64};
-  static const int kGrabs[] = {4, 8, 16};
+  static const int kGrabs[] = {4, 8, 16, 32};
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
     if (e0) cudaEventDestroy(e0);

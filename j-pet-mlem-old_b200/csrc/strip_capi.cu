@@ -811,13 +811,13 @@ int adjoint_dev(strip_ctx* ctx, const double* d_w, double sz, double sdl,
   CK(cudaMemsetAsync(d_g, 0, ctx->n_pix * sizeof(double), ctx->stream));
   // the weights in binned order (read contiguously by the kernels)
   if (!ctx->d_wbin && ctx->n_binned > 0)
-    CK(cudaMalloc(&ctx->d_wbin, ctx->n_binned * sizeof(double)));
+    CK(cudaMalloc(&ctx->d_wbin, ctx->n_binned * sizeof(float)));
   CK(launch_gather_weights(ctx->d_perm, d_w, ctx->n_binned, ctx->d_wbin,
                            ctx->stream));
   LaunchArgs a = base_args(ctx);
   a.k = make_kernel(sz, sdl, ctx->s.pw);
   a.acc = d_g;
-  a.w_in = ctx->d_wbin;
+  a.wf_in = ctx->d_wbin;
   // GaussianKernel values are at most kc / sqrt(2 R^2 ipsz): E <= 1 and
   // a'Sa >= ipsz (ap^2 + aq^2) >= 2 R^2 ipsz sec^4
   a.kbound = (float)((double)a.k.kc /

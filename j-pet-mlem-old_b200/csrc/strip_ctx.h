@@ -26,9 +26,9 @@ struct strip_ctx {
   double* d_acc_own = nullptr;  // the context's own accumulator
   int acc_mode = STRIP_MODE_CPU;  // mode of the last strip_accumulate
   int tile_pref = 32;  // tile edge in pixels (autotuned or 32)
-  int grab = 16;       // events a warp takes per counter step (autotuned or 16)
+  int grab = 32;       // events a warp takes per counter step (autotuned or 32)
   float* d_sens5 = nullptr;
-  double* d_wbin = nullptr;     // adjoint weights in binned order (n_binned)
+  float* d_wbin = nullptr;  // adjoint weights in binned order (n_binned, binary32)
   // binned events
   int64_t n_events = 0;   // as given by the caller
   int64_t n_binned = 0;   // events with a non-empty box

@@ -103,8 +103,8 @@ struct LaunchArgs {
   int64_t g_begin;       // global-path event range [g_begin, g_begin+g_count)
   int64_t g_count;
   double* y_out;         // OP_FORWARD: per event (caller order)
-  const double* w_in;    // OP_ADJOINT: per event weights in binned order;
-                         // OP_GRAD: in the caller's order
+  const double* w_in;    // OP_GRAD: per event weights in the caller's order
+  const float* wf_in;    // OP_ADJOINT: per event weights in binned order
   double* grad_out;      // OP_GRAD: 2 doubles (atomic)
   double sz, sdl;        // OP_GRAD: model sigmas
   float kbound;          // bound of the GaussianKernel values (OP_ADJOINT,
@@ -180,9 +180,10 @@ cudaError_t launch_update_out(const float* rho_in, float* rho_out,
                               cudaStream_t st);
 // Whether MLEM in `mode` accumulates rho-weighted contributions.
 inline int mlem_weighted(int mode) { return mode == STRIP_MODE_CPU; }
-// out_i = w[perm_i]: caller-order weights into binned order
+// out_i = w[perm_i]: caller-order weights into binned order (binary32, the
+// precision the adjoint scales its kernel values with)
 cudaError_t launch_gather_weights(const int64_t* perm, const double* w,
-                                  int64_t n, double* out, cudaStream_t st);
+                                  int64_t n, float* out, cudaStream_t st);
 // Sets the batched tile kernel's dynamic shared-memory limit (before a
 // launch is captured into a graph).
 cudaError_t tile_batch_reserve_smem(int mode, int accum, int smem_bytes);

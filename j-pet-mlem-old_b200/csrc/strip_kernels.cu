@@ -531,13 +531,14 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
 struct EventAux {
   int64_t out = 0;
   double w = 0.0;
+  float wf = 0.0f;
 };
 
 template <int OP>
 __device__ __forceinline__ EventAux load_aux(const LaunchArgs& a, int64_t pos) {
   EventAux x;
   if constexpr (OP == OP_FORWARD) x.out = a.perm[pos];
-  if constexpr (OP == OP_ADJOINT) x.w = a.w_in[pos];
+  if constexpr (OP == OP_ADJOINT) x.wf = a.wf_in[pos];
   if constexpr (OP == OP_GRAD) x.w = a.w_in[a.perm[pos]];
   return x;
 }
@@ -546,8 +547,8 @@ template <int OP>
 __device__ __forceinline__ EventAux shfl_aux(const EventAux& m, int src) {
   EventAux x;
   if constexpr (OP == OP_FORWARD) x.out = __shfl_sync(kFull, m.out, src);
-  if constexpr (OP == OP_ADJOINT || OP == OP_GRAD)
-    x.w = __shfl_sync(kFull, m.w, src);
+  if constexpr (OP == OP_ADJOINT) x.wf = __shfl_sync(kFull, m.wf, src);
+  if constexpr (OP == OP_GRAD) x.w = __shfl_sync(kFull, m.w, src);
   return x;
 }
 
@@ -627,7 +628,7 @@ __device__ __forceinline__ float process_event(const LaunchArgs& a,
     if (!(D > 0.0)) return 0.0f;
     scale = rcp_approx((float)D);  // within an ulp of 1 / D; 0 or inf at the range ends
   } else {
-    scale = (float)aux.w;  // OP_ADJOINT
+    scale = aux.wf;  // OP_ADJOINT
     if (scale == 0.0f) return 0.0f;
   }
   if constexpr (Win::unweighted()) {
@@ -671,7 +672,7 @@ __device__ int adjoint_shift(const LaunchArgs& a, const WorkItem& it, int lane) 
   float m = 0.0f;
   for (int64_t i = it.begin + threadIdx.x; i < it.begin + it.count;
        i += blockDim.x)
-    m = fmaxf(m, fabsf((float)a.w_in[i]));
+    m = fmaxf(m, fabsf(a.wf_in[i]));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(kFull, m, o));
   if (lane == 0) s_wmax[threadIdx.x >> 5] = m;
@@ -1065,10 +1066,10 @@ __global__ void k_bin_scatter(const int* keys, int64_t n, const float* zu,
 }
 
 __global__ void k_gather_weights(const int64_t* perm, const double* w,
-                                 int64_t n, double* out) {
+                                 int64_t n, float* out) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = w[perm[i]];
+    out[i] = (float)w[perm[i]];
 }
 
 __global__ void k_update_out(const float* rho_in, float* rho_out,
@@ -1369,7 +1370,7 @@ cudaError_t launch_update(float* rho, double* acc, int64_t n_pix, double scale,
 }
 
 cudaError_t launch_gather_weights(const int64_t* perm, const double* w,
-                                  int64_t n, double* out, cudaStream_t st) {
+                                  int64_t n, float* out, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   k_gather_weights<<<grid_for(n), kThreads, 0, st>>>(perm, w, n, out);
   return cudaGetLastError();

@@ -240,7 +240,7 @@ class Reconstruction:
         self.n_subsets = 1
         return {"tile": t.tile, "grab": t.grab, "ms": t.ms}
 
-    def set_schedule(self, tile=32, grab=8):
+    def set_schedule(self, tile=32, grab=32):
         self._check(self.lib.strip_set_schedule(self._ctx, int(tile), int(grab)))
 
     # -- split iteration (events sharded over processes) -------------------
