@@ -299,6 +299,10 @@ __device__ __forceinline__ void build_lane_rows_t(const ScannerF& s,
 #pragma unroll
   for (int b = 0; b < kRowBlocks; ++b) {
     L.run[b] = 0u;
+    if constexpr (MODE == STRIP_MODE_CPU) {  // rows without a run walk nothing
+      L.K0[b] = 0.0f;
+      L.R0[b] = 0.0f;
+    }
     const int i = rank0 + 32 * b + lane;
     if (i < H) {
       const int iy = e.tly + ranked_row(H, i);
@@ -352,7 +356,9 @@ __device__ __forceinline__ void pass1_rows(const ScannerF& s, const KernelF& k,
 #pragma unroll
   for (int b = 0; b < kRowBlocks; ++b) {
     const int n = run_len(L.run[b]);
-    if (b < nb && n > 0) {
+    // every lane enters (a lane without a run walks n = 0 pixels): the warp
+    // stays converged instead of branching around empty rows
+    if (b < nb) {
       const auto p = win.run_ptr(L.run[b], e, H, rank0 + 32 * b + lane);
       float a = 0.0f;
       if constexpr (MODE == STRIP_MODE_CPU && kPairs && Win::kShared) {
@@ -422,7 +428,9 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
 #pragma unroll
   for (int b = 0; b < kRowBlocks; ++b) {
     const int n = run_len(L.run[b]);
-    if (b < nb && n > 0) {
+    // every lane enters (a lane without a run walks n = 0 pixels): the warp
+    // stays converged instead of branching around empty rows
+    if (b < nb) {
       const auto p = win.run_ptr(L.run[b], e, H, rank0 + 32 * b + lane);
       if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED && Win::unweighted()) {
         // K / D in fixed point: no image reads, one conversion per pixel
