@@ -489,8 +489,9 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
         }
       } else if constexpr (MODE == STRIP_MODE_CPU && kPairs && Win::pair_add()) {
         // the adjoint's signed fixed point: K_j w_e with w_e and the unit
-        // folded into the run's first value, two pixels a step, one
-        // conversion per pixel
+        // folded into the run's first value, two pixels a step; rounding by
+        // the 1.5 * 2^23 addend (|addend| < 2^22: round to nearest even, as
+        // cvt.rni) keeps the conversions off the MUFU/conversion pipe
         const float K0 = L.K0[b] * sc, R0 = L.R0[b], R2 = R0 * R0;
         float2 P = make_float2(K0, K0 * R0);
         float2 S = make_float2(R2 * k.q, R2 * k.q3);
@@ -498,8 +499,9 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
         uint32_t aa = win.acc_addr(p);
 #pragma unroll 2
         for (int c = n >> 1; c > 0; --c, aa += 8) {
-          red_shared_add(aa, (unsigned)__float2int_rn(P.x));
-          red_shared_add(aa + 4, (unsigned)__float2int_rn(P.y));
+          const float2 x = __fadd2_rn(P, make_float2(kMagicSigned, kMagicSigned));
+          red_shared_add(aa, __float_as_uint(x.x) - kMagicSignedBits);
+          red_shared_add(aa + 4, __float_as_uint(x.y) - kMagicSignedBits);
           P = __fmul2_rn(P, S);
           S = __fmul2_rn(S, Q4);
         }
