@@ -247,7 +247,7 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
   CKB(cudaMemcpyAsync(d_hist, offs.data(), n_keys * sizeof(unsigned long long),
                       cudaMemcpyHostToDevice, st));
   CKB(launch_bin_scatter(keys, n, zu, zd, dl, orig, d_hist, ozu, ozd, odl,
-                         operm, st));
+                         operm, n_keys, st));
 
   // Work items: chunks of each (subset, tile) bin, sized for >= ~8 waves and
   // at most kMaxItemEvents events (the fixed-point window accumulator's

@@ -165,7 +165,7 @@ cudaError_t launch_bin_scatter(const int* keys, int64_t n, const float* zu,
                                const int64_t* orig,
                                unsigned long long* cursor, float* ozu,
                                float* ozd, float* odl, int64_t* operm,
-                               cudaStream_t st);
+                               int64_t n_keys, cudaStream_t st);
 cudaError_t launch_tile(int op, int mode, int accum, const LaunchArgs& a,
                         cudaStream_t st);
 cudaError_t launch_global(int op, int mode, int accum, const LaunchArgs& a,

@@ -1020,9 +1020,14 @@ __global__ void k_event_boxes(ScannerF s, const float* zu, const float* zd,
 
 // key = subset * (n_tiles + 1) + tile, tile == n_tiles for the global path,
 // -1 for an empty box.
+// Keys and their histogram; with n_local > 0 (the number of keys) the CTA
+// counts in shared memory first and adds its counts once per key.
 __global__ void k_bin_keys(Tiling t, int n_z, int n_y, const int4* boxes,
                            const int64_t* orig, int64_t n, int n_subsets,
-                           int* keys, unsigned long long* hist) {
+                           int* keys, unsigned long long* hist, int n_local) {
+  extern __shared__ unsigned s_hist[];
+  for (int k = threadIdx.x; k < n_local; k += blockDim.x) s_hist[k] = 0u;
+  if (n_local > 0) __syncthreads();
   const int lane = threadIdx.x & 31;
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwt = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -1043,17 +1048,70 @@ __global__ void k_bin_keys(Tiling t, int n_z, int n_y, const int4* boxes,
       keys[i] = key;
     }
     const unsigned peers = __match_any_sync(kFull, key);
-    if (key >= 0 && lane == __ffs(peers) - 1)
-      atomicAdd(hist + key, (unsigned long long)__popc(peers));
+    if (key >= 0 && lane == __ffs(peers) - 1) {
+      if (n_local > 0)
+        atomicAdd(s_hist + key, (unsigned)__popc(peers));
+      else
+        atomicAdd(hist + key, (unsigned long long)__popc(peers));
+    }
+  }
+  if (n_local > 0) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < n_local; k += blockDim.x)
+      if (s_hist[k]) atomicAdd(hist + k, (unsigned long long)s_hist[k]);
   }
 }
 
+// Scatters the events into their bins.  With n_local > 0 (the number of
+// keys) each CTA takes a contiguous chunk, counts its keys in shared memory,
+// reserves its slots with one global atomic per key, and places events from
+// shared-memory offsets; otherwise one warp-aggregated global atomic per key
+// and warp.
 __global__ void k_bin_scatter(const int* keys, int64_t n, const float* zu,
                               const float* zd, const float* dl,
                               const int64_t* orig, unsigned long long* cursor,
                               float* ozu, float* ozd, float* odl,
-                              int64_t* operm) {
+                              int64_t* operm, int n_local) {
   const int lane = threadIdx.x & 31;
+  auto place = [&](int64_t i, int64_t p) {
+    ozu[p] = zu[i];
+    ozd[p] = zd[i];
+    odl[p] = dl[i];
+    operm[p] = orig ? orig[i] : i;
+  };
+  if (n_local > 0) {
+    extern __shared__ unsigned long long s_base[];  // n_local bases, then counts
+    unsigned* s_cnt = reinterpret_cast<unsigned*>(s_base + n_local);
+    const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t c0 = (int64_t)blockIdx.x * chunk;
+    const int64_t c1 = min(n, c0 + chunk);
+    for (int k = threadIdx.x; k < n_local; k += blockDim.x) s_cnt[k] = 0u;
+    __syncthreads();
+    for (int64_t base = c0 + (threadIdx.x & ~31); base < c1; base += blockDim.x) {
+      const int64_t i = base + lane;
+      const int key = i < c1 ? keys[i] : -1;
+      const unsigned peers = __match_any_sync(kFull, key);
+      if (key >= 0 && lane == __ffs(peers) - 1) atomicAdd(s_cnt + key, (unsigned)__popc(peers));
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < n_local; k += blockDim.x) {
+      s_base[k] = s_cnt[k] ? atomicAdd(cursor + k, (unsigned long long)s_cnt[k]) : 0ull;
+      s_cnt[k] = 0u;
+    }
+    __syncthreads();
+    for (int64_t base = c0 + (threadIdx.x & ~31); base < c1; base += blockDim.x) {
+      const int64_t i = base + lane;
+      const int key = i < c1 ? keys[i] : -1;
+      const unsigned peers = __match_any_sync(kFull, key);
+      const int leader = __ffs(peers) - 1;
+      unsigned o = 0;
+      if (key >= 0 && lane == leader) o = atomicAdd(s_cnt + key, (unsigned)__popc(peers));
+      o = __shfl_sync(kFull, o, leader);
+      if (key >= 0)
+        place(i, (int64_t)s_base[key] + o + __popc(peers & ((1u << lane) - 1u)));
+    }
+    return;
+  }
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwt = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t base = wid * 32; base < n; base += nwt * 32) {
@@ -1065,13 +1123,7 @@ __global__ void k_bin_scatter(const int* keys, int64_t n, const float* zu,
     if (key >= 0 && lane == leader)
       p0 = atomicAdd(cursor + key, (unsigned long long)__popc(peers));
     p0 = __shfl_sync(kFull, p0, leader);
-    if (key >= 0) {
-      const int64_t p = (int64_t)p0 + __popc(peers & ((1u << lane) - 1u));
-      ozu[p] = zu[i];
-      ozd[p] = zd[i];
-      odl[p] = dl[i];
-      operm[p] = orig ? orig[i] : i;
-    }
+    if (key >= 0) place(i, (int64_t)p0 + __popc(peers & ((1u << lane) - 1u)));
   }
 }
 
@@ -1356,8 +1408,11 @@ cudaError_t launch_bin_keys(const Tiling& t, int n_z, int n_y,
                             int n_subsets, int* keys, unsigned long long* hist,
                             cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  k_bin_keys<<<grid_for(n), kThreads, 0, st>>>(t, n_z, n_y, boxes, orig, n,
-                                               n_subsets, keys, hist);
+  // per-CTA counts in shared memory up to 12288 keys (48 KB)
+  const int64_t n_keys = (int64_t)n_subsets * (t.n_tiles + 1);
+  const int n_local = n_keys <= 12288 ? (int)n_keys : 0;
+  k_bin_keys<<<grid_for(n), kThreads, n_local * sizeof(unsigned), st>>>(
+      t, n_z, n_y, boxes, orig, n, n_subsets, keys, hist, n_local);
   return cudaGetLastError();
 }
 
@@ -1365,10 +1420,12 @@ cudaError_t launch_bin_scatter(const int* keys, int64_t n, const float* zu,
                                const float* zd, const float* dl,
                                const int64_t* orig, unsigned long long* cursor,
                                float* ozu, float* ozd, float* odl,
-                               int64_t* operm, cudaStream_t st) {
+                               int64_t* operm, int64_t n_keys, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  k_bin_scatter<<<grid_for(n), kThreads, 0, st>>>(keys, n, zu, zd, dl, orig,
-                                                  cursor, ozu, ozd, odl, operm);
+  // per-CTA reservations in shared memory up to 4096 keys (48 KB)
+  const int n_local = n_keys <= 4096 ? (int)n_keys : 0;
+  k_bin_scatter<<<grid_for(n), kThreads, n_local * 12, st>>>(
+      keys, n, zu, zd, dl, orig, cursor, ozu, ozd, odl, operm, n_local);
   return cudaGetLastError();
 }
 
