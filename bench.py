@@ -47,8 +47,8 @@ PHANTOM = [
 SEED = 20260101
 # DRAM bytes (read + write) per event of one k_tile pass, from an ncu capture
 # of this workload's first 2e7 events (profiles/k_tile_strip_c2_2e7events.md:
-# 245.1 MB read + 5.4 MB written); the traffic grows with the event count.
-TILE_DRAM_BYTES_PER_EVENT = (245.074176e6 + 5.365504e6) / 2e7
+# 245.0 MB read + 6.7 MB written); the traffic grows with the event count.
+TILE_DRAM_BYTES_PER_EVENT = (244.954880e6 + 6.694656e6) / 2e7
 
 
 def workload_config(n_events, e2e_iters, world=1):
