@@ -212,6 +212,73 @@ SIGNATURES = {
     ),
 }
 
+
+
+class HybridSetup(ctypes.Structure):
+    """hybrid_setup of include/hybridmlem.h."""
+    _fields_ = [
+        ("n_columns", ctypes.c_int32),
+        ("n_rows", ctypes.c_int32),
+        ("n_planes", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("pixel_size", ctypes.c_double),
+        ("z_left", ctypes.c_double),
+        ("length", ctypes.c_double),
+        ("sigma_z", ctypes.c_double),
+        ("sigma_dl", ctypes.c_double),
+    ]
+
+
+class HybridStats(ctypes.Structure):
+    """hybrid_stats of include/hybridmlem.h."""
+    _fields_ = [
+        ("n_responses", ctypes.c_int64),
+        ("n_events", ctypes.c_int64),
+        ("n_lors", ctypes.c_int64),
+        ("n_pixel_infos", ctypes.c_int64),
+        ("used_pixels", ctypes.c_int64),
+        ("used_voxels", ctypes.c_int64),
+        ("iterations", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("last_iteration_ms", ctypes.c_double),
+    ]
+
+
+class HybridCylinder(ctypes.Structure):
+    """hybrid_cylinder of include/hybridmlem.h."""
+    _fields_ = [(k, ctypes.c_double) for k in
+                ("x", "y", "z", "radius", "half_length", "activity")]
+
+
+HYBRID_SENS_CALCULATE, HYBRID_SENS_ONE, HYBRID_SENS_EXTERNAL = 0, 1, 2
+HYBRID_PROGRESS_CB = ctypes.CFUNCTYPE(None, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p)
+_vp = ctypes.c_void_p
+
+# every symbol include/hybridmlem.h declares
+SIGNATURES.update({
+    "hybrid_ctx_create": (ctypes.c_int, [_P(HybridSetup), ctypes.c_int32, _P(ctypes.c_void_p)]),
+    "hybrid_ctx_destroy": (ctypes.c_int, [_ctx]),
+    "hybrid_last_error": (ctypes.c_char_p, [_ctx]),
+    "hybrid_set_geometry_from_matrix": (
+        ctypes.c_int,
+        [_ctx, ctypes.c_int32, _vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp, ctypes.c_uint32,
+         _vp, ctypes.c_int32]),
+    "hybrid_get_geometry": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "hybrid_set_sensitivity": (ctypes.c_int, [_ctx, ctypes.c_int32, _vp]),
+    "hybrid_get_sensitivity": (ctypes.c_int, [_ctx, _vp]),
+    "hybrid_set_responses": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp, _vp, ctypes.c_int64]),
+    "hybrid_get_frames": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "hybrid_iterate": (ctypes.c_int, [_ctx, ctypes.c_int32, HYBRID_PROGRESS_CB, _vp]),
+    "hybrid_set_image": (ctypes.c_int, [_ctx, _vp]),
+    "hybrid_get_image": (ctypes.c_int, [_ctx, _vp]),
+    "hybrid_get_stats": (ctypes.c_int, [_ctx, _P(HybridStats)]),
+    "hybrid_generate_responses": (
+        ctypes.c_int,
+        [ctypes.c_int32, _vp, _P(HybridCylinder), ctypes.c_int32, ctypes.c_double,
+         ctypes.c_double, ctypes.c_double, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int32,
+         _vp, _vp, _vp, _vp, _vp]),
+})
+
 _lib = None
 
 
