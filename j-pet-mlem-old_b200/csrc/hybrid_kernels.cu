@@ -2,44 +2,105 @@
 //
 // One warp per frame event.  The event's voxels are its LOR pixel infos
 // [info_begin, info_end) times its planes [plane_begin, plane_end); the warp
-// walks them flattened with the plane fastest, so that 32 lanes cover a few
-// pixels x consecutive planes.  The volume is held on the device with the
-// plane index fastest (z-fast: voxel (x, y, z) at (x + n_c y) n_p + z), so a
-// warp's image reads and its accumulator atomics fall on a few contiguous
-// sectors instead of 32 scattered ones; the boundary layout (x fastest) is
-// restored by launch_from_zfast.
+// walks them flattened with the plane fastest.  The volume is held on the
+// device with the plane index fastest (z-fast: voxel (x, y, z) at
+// (x + n_c y) n_p + z), so a warp's image reads and accumulator atomics fall
+// on a few contiguous sectors; the boundary layout (x fastest) is restored
+// by launch_from_zfast.
 //
 // Per voxel (GaussianKernel::normalized, src/2d/strip/gaussian_kernel.h:
 // 51-105, in the frame of the event's LOR):
 //   K = c / sqrt(a' S a) exp(-b' S b / 2) / sens(z, up),
 //   sens = (atan u - atan v) / pi,  weight = K w rho,  D += weight s.
-// Everything that depends on the pixel only (a' S a, the b_r term, 1/(R -+ up),
-// the LOR weight and the pixel's sensitivity) is computed once per pixel into
-// the warp's shared memory; per voxel remain one exp, one atan2 (the
-// difference of the two arctangents: atan u - atan v = atan2(u - v, 1 + u v),
-// whose sign is that of u - v, as the reference's) and a division.  Pass 1
-// keeps each voxel's weight in a per-warp shared cache (first kCache voxels);
-// pass 2 scatters weight / D with one red.global.add.f32 per voxel, reading
-// the cache or recomputing past it.
+// Everything that depends on the pixel only (c / sqrt(a' S a) w, (up_p - up)
+// tan, the b_r term, 1 / (R -+ up_p), the pixel's sensitivity and its base
+// index) is computed once per pixel into the warp's shared memory; per voxel
+// remain z, the two ratios of the sensitivity (from z exactly as the
+// reference forms them, so the decisions sens <= 0 at z = +-L/2 are the
+// reference's), one exp2, the arctangent difference atan u - atan v =
+// atan2(u - v, 1 + u v) by atan2_pos below, and an image load.  (A table of
+// 1 / sens per pixel info and plane -- it depends on the LOR, the pixel and
+// the plane only -- was slower: 414 against 252 ms per iteration on the
+// big-barrel workload, the walk waiting on its HBM loads.)  Pass 1 keeps each
+// voxel's weight in a per-warp shared cache (first kCache voxels); pass 2
+// scatters weight / D with one red.global.add.f32 per voxel, reading the
+// cache or recomputing past it.
 #include "hybrid_internal.h"
 
 namespace hybridmlem {
 
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
-constexpr int kCache = 2048;        // cached voxel weights per warp
-constexpr int kBlocksPerSm = 3;     // 3 x (8 warps x 8.9 KB) of shared memory
+// Launch shape and per-warp cache (compile-time tuning constants).
+#ifndef HYBRID_WARPS
+#define HYBRID_WARPS 8
+#endif
+#ifndef HYBRID_CACHE
+#define HYBRID_CACHE 2048
+#endif
+#ifndef HYBRID_BLOCKS_PER_SM
+#define HYBRID_BLOCKS_PER_SM 3
+#endif
+constexpr int kWarps = HYBRID_WARPS;
+constexpr int kThreads = kWarps * 32;
+constexpr int kCache = HYBRID_CACHE;          // cached voxel weights per warp
+constexpr int kBlocksPerSm = HYBRID_BLOCKS_PER_SM;
 
+// atan2(a, b) for a > 0, in (0, pi): the quotient of the smaller by the
+// larger of a and |b| (fast division) folded into [0, 1], an odd polynomial
+// t P(t^2) of degree 15 for atan on [0, 1] (coefficients fitted for this
+// kernel by iteratively reweighted least squares toward the minimax absolute
+// error: 3.8e-8 in exact arithmetic, 1.1e-7 evaluated in binary32), then the
+// quadrant.  The reference's atanf(u) - atanf(v) carries about the same
+// binary32 rounding.
+__device__ __forceinline__ float atan2_pos(float a, float b) {
+  const float ab = fabsf(b);
+  const float mx = fmaxf(a, ab), mn = fminf(a, ab);
+  const float t = __fdividef(mn, mx);
+  const float s = t * t;
+  float p = -0.004054941702634096f;
+  p = fmaf(p, s, 0.021864276379346848f);
+  p = fmaf(p, s, -0.055914171040058136f);
+  p = fmaf(p, s, 0.09642327576875687f);
+  p = fmaf(p, s, -0.1390867829322815f);
+  p = fmaf(p, s, 0.19946575164794922f);
+  p = fmaf(p, s, -0.33329862356185913f);
+  p = fmaf(p, s, 0.9999993443489075f);
+  float r = t * p;
+  if (a > ab) r = 1.5707963267948966f - r;
+  if (b < 0.0f) r = 3.14159265358979f - r;
+  return r;
+}
+
+// z of plane iz (VoxelGrid::center_z_at, voxel_grid.h:38-40).
+__device__ __forceinline__ float plane_z(const GridF& g, int iz) {
+  return ((float)iz + 0.5f) * g.p + g.z_left;
+}
+
+// pi / (pi sens) of a voxel at z for a pixel at up_p in a LOR of half length
+// R (GaussianKernel::sensitivity, gaussian_kernel.h:139-148, with the two
+// quotients as products by 1 / (R -+ up_p)); 0 where sens <= 0.  The signs
+// of the two ratios, hence the decision sens <= 0, are the reference's.
+__device__ __forceinline__ float inv_sens(float half_L, float z, float ra, float rb) {
+  const float lmz = half_L - z, lpz = half_L + z;
+  const float u = fminf(lmz * ra, lpz * rb);
+  const float v = fmaxf(-lpz * ra, -lmz * rb);
+  const float a = u - v;
+  if (!(a > 0.0f)) return 0.0f;
+  return __fdividef(3.14159265358979f, atan2_pos(a, fmaf(u, v, 1.0f)));
+}
+
+__device__ __forceinline__ float proj_up(const GridF& g, short2 p, float4 md) {
+  const float cx = g.llc_x + (float)p.x * g.p;
+  const float cy = g.llc_y + (float)p.y * g.p;
+  return (cx - md.x) * md.z + (cy - md.y) * md.w;
+}
+
+// Event-dependent pixel terms of one chunk of 32 pixel infos.
 struct PixelData {
-  float bw[32];   // c / sqrt(a' S a) * w
-  float dy[32];   // up_pixel - up
-  float brr[32];  // b_r S_dl b_r
-  float ra[32];   // 1 / (R - up_pixel)
-  float rb[32];   // 1 / (R + up_pixel)
-  float s[32];    // sensitivity of the pixel
-  int vbase[32];  // z-fast index of the pixel's plane 0
+  float4 t[32];    // c / sqrt(a' S a) w, (up_p - up) tan, b_r S_dl b_r, s
+  float2 r[32];    // 1 / (R - up_p), 1 / (R + up_p)
+  int base[32];    // z-fast index of plane 0
 };
 
 struct WarpSmem {
@@ -47,7 +108,6 @@ struct WarpSmem {
   float cache[kCache];
 };
 
-// Per-pixel terms of the chunk [c0, c0 + 32) of the event's pixel infos.
 __device__ __forceinline__ void load_pixels(const GridF& g, const GeometryDev& geo,
                                             const float* __restrict__ sens, const Frame& f,
                                             float4 md, float R, int c0, int n_pix, int lane,
@@ -57,10 +117,7 @@ __device__ __forceinline__ void load_pixels(const GridF& g, const GeometryDev& g
     const int64_t info = (int64_t)f.info_begin + k;
     const short2 p = geo.pix[info];
     const float w = geo.w[info];
-    // PixelGrid::center_at and projection_relative_middle
-    const float cx = g.llc_x + (float)p.x * g.p;
-    const float cy = g.llc_y + (float)p.y * g.p;
-    const float upp = (cx - md.x) * md.z + (cy - md.y) * md.w;
+    const float upp = proj_up(g, p, md);
     const float dy = upp - f.up;
     const float yp = dy + f.up;
     const float sec_sq = f.sec * f.sec;
@@ -70,39 +127,32 @@ __device__ __forceinline__ void load_pixels(const GridF& g, const GeometryDev& g
     const float aca = ap * g.ipz * ap + aq * g.ipz * aq + ar * g.ipdl * ar;
     const float br = -2.0f * dy * f.sec;
     const int pidx = p.x + g.nc * p.y;
-    px.bw[lane] = g.norm_c / sqrtf(aca) * w;
-    px.dy[lane] = dy;
-    px.brr[lane] = br * g.ipdl * br;
-    px.ra[lane] = 1.0f / (R - upp);
-    px.rb[lane] = 1.0f / (R + upp);
-    px.s[lane] = sens[pidx];
-    px.vbase[lane] = pidx * g.np;
+    px.t[lane] = make_float4(g.norm_c * rsqrtf(aca) * w, dy * f.tan, br * g.ipdl * br,
+                             sens[pidx]);
+    px.r[lane] = make_float2(__frcp_rn(R - upp), __frcp_rn(R + upp));
+    px.base[lane] = pidx * g.np;
   }
   __syncwarp();
 }
 
-// K w (without rho) of voxel (pixel j of the chunk, plane iz); 0 where the
-// normalised kernel is not positive.
+// K w (without rho) of voxel (pixel j of the chunk, plane iz).
 __device__ __forceinline__ float voxel_kw(const GridF& g, const Frame& f, const PixelData& px,
                                           int j, int iz, float half_L) {
-  const float z = ((float)iz + 0.5f) * g.p + g.z_left;
-  const float dx = z - f.right;
-  const float bpq = dx - px.dy[j] * f.tan;
+  const float4 t4 = px.t[j];
+  const float z = plane_z(g, iz);
+  const float2 r = px.r[j];
+  const float is = inv_sens(half_L, z, r.x, r.y);
+  if (is == 0.0f) return 0.0f;
+  const float bpq = (z - f.right) - t4.y;
   const float t = bpq * g.ipz * bpq;
-  const float bcb = (t + t) + px.brr[j];
-  const float e = __expf(-0.5f * bcb);
-  const float ra = px.ra[j], rb = px.rb[j];
-  const float u = fminf((half_L - z) * ra, (half_L + z) * rb);
-  const float v = fmaxf(-(half_L + z) * ra, (z - half_L) * rb);
-  const float th = atan2f(u - v, fmaf(u, v, 1.0f));
-  if (!(th > 0.0f)) return 0.0f;
-  return px.bw[j] * e * (3.14159265358979f / th);
+  const float bcb = (t + t) + t4.z;
+  return t4.x * exp2f(-0.7213475204444817f * bcb) * is;  // exp(-bcb / 2)
 }
 
 __global__ void __launch_bounds__(kThreads, kBlocksPerSm)
 k_mlem(const GridF g, const GeometryDev geo, const float* __restrict__ sens,
-       const Frame* __restrict__ frames, int64_t n_frames, const float* __restrict__ rho_t,
-       float* acc_t) {
+       const Frame* __restrict__ frames, int64_t n_frames,
+       const float* __restrict__ rho_t, float* acc_t) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -117,20 +167,20 @@ k_mlem(const GridF g, const GeometryDev geo, const float* __restrict__ sens,
     const float4 md = geo.lor_md[f.lor];
     const float R = geo.lor_len[f.lor] / 2;
     const int q = 32 / n_pl, r = 32 - q * n_pl;
+    const int j0 = lane / n_pl, pz0 = lane - j0 * n_pl;
     // pass 1: weights and the denominator
     float d = 0.0f;
     for (int c0 = 0; c0 < n_pix; c0 += 32) {
       load_pixels(g, geo, sens, f, md, R, c0, n_pix, lane, sm.px);
-      const int cn = min(32, n_pix - c0);
-      const int nv = cn * n_pl;
+      const int nv = min(32, n_pix - c0) * n_pl;
       const int base = c0 * n_pl;
-      int j = lane / n_pl, pz = lane - (lane / n_pl) * n_pl;
+      int j = j0, pz = pz0;
       for (int v = lane; v < nv; v += 32) {
         const int iz = f.plane_begin + pz;
         float wgt = voxel_kw(g, f, sm.px, j, iz, half_L);
         if (wgt != 0.0f) {
-          wgt *= __ldg(rho_t + sm.px.vbase[j] + iz);
-          d += wgt * sm.px.s[j];
+          wgt *= __ldg(rho_t + sm.px.base[j] + iz);
+          d = fmaf(wgt, sm.px.t[j].w, d);
         }
         if (base + v < kCache) sm.cache[base + v] = wgt;
         j += q;
@@ -150,22 +200,20 @@ k_mlem(const GridF g, const GeometryDev geo, const float* __restrict__ sens,
     // pass 2: scatter weight / D
     for (int c0 = 0; c0 < n_pix; c0 += 32) {
       const int base = c0 * n_pl;
-      const int cn = min(32, n_pix - c0);
-      const int nv = cn * n_pl;
-      const bool cached = base + nv <= kCache;
-      if (cached) {
-        if (lane < cn) {
+      const int nv = min(32, n_pix - c0) * n_pl;
+      if (base + nv <= kCache) {
+        if (c0 + lane < n_pix) {
           const short2 p = geo.pix[(int64_t)f.info_begin + c0 + lane];
-          sm.px.vbase[lane] = (p.x + g.nc * p.y) * g.np;
+          sm.px.base[lane] = (p.x + g.nc * p.y) * g.np;
         }
         __syncwarp();
       } else {
         load_pixels(g, geo, sens, f, md, R, c0, n_pix, lane, sm.px);
       }
-      int j = lane / n_pl, pz = lane - (lane / n_pl) * n_pl;
+      int j = j0, pz = pz0;
       for (int v = lane; v < nv; v += 32) {
         const int iz = f.plane_begin + pz;
-        const int vi = sm.px.vbase[j] + iz;
+        const int vi = sm.px.base[j] + iz;
         float wgt;
         if (base + v < kCache) {
           wgt = sm.cache[base + v];
@@ -243,9 +291,9 @@ void launch_from_zfast(const GridF& g, const float* rho_t, float* rho, cudaStrea
   k_from_zfast<<<grid_for((int64_t)g.n_pixels * g.np), 256, 0, st>>>(g, rho_t, rho);
 }
 
-void launch_mlem(const GridF& g, const GeometryDev& geo, const float* sens,
-                 const Frame* frames, int64_t n_frames, const float* rho_t, float* acc_t,
-                 int n_blocks, cudaStream_t st) {
+void launch_mlem(const GridF& g, const GeometryDev& geo, const float* sens, const Frame* frames,
+                 int64_t n_frames, const float* rho_t, float* acc_t, int n_blocks,
+                 cudaStream_t st) {
   const int smem = (int)sizeof(WarpSmem) * kWarps;
   cudaFuncSetAttribute(k_mlem, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   k_mlem<<<n_blocks, kThreads, smem, st>>>(g, geo, sens, frames, n_frames, rho_t, acc_t);

@@ -175,3 +175,4 @@ def test_device_generator_equals_host_generator():
     assert same.mean() > 0.999  # libm and CUDA sin / cos / log may round apart
     for a, c in zip(h[2:], d[2:]):
         assert np.allclose(a[same], c[same], rtol=0, atol=1e-5)
+
