@@ -41,10 +41,14 @@ namespace {
 #ifndef HYBRID_BLOCKS_PER_SM
 #define HYBRID_BLOCKS_PER_SM 3
 #endif
+#ifndef HYBRID_UNROLL
+#define HYBRID_UNROLL 1
+#endif
 constexpr int kWarps = HYBRID_WARPS;
 constexpr int kThreads = kWarps * 32;
 constexpr int kCache = HYBRID_CACHE;          // cached voxel weights per warp
 constexpr int kBlocksPerSm = HYBRID_BLOCKS_PER_SM;
+constexpr int kUnroll = HYBRID_UNROLL;           // voxel-loop unroll
 
 // atan2(a, b) for a > 0, in (0, pi): the quotient of the smaller by the
 // larger of a and |b| (fast division) folded into [0, 1], an odd polynomial
@@ -175,11 +179,14 @@ k_mlem(const GridF g, const GeometryDev geo, const float* __restrict__ sens,
       const int nv = min(32, n_pix - c0) * n_pl;
       const int base = c0 * n_pl;
       int j = j0, pz = pz0;
+#pragma unroll kUnroll
       for (int v = lane; v < nv; v += 32) {
         const int iz = f.plane_begin + pz;
+        // the image load goes out first; the kernel arithmetic hides it
+        const float rho = __ldg(rho_t + sm.px.base[j] + iz);
         float wgt = voxel_kw(g, f, sm.px, j, iz, half_L);
         if (wgt != 0.0f) {
-          wgt *= __ldg(rho_t + sm.px.base[j] + iz);
+          wgt *= rho;
           d = fmaf(wgt, sm.px.t[j].w, d);
         }
         if (base + v < kCache) sm.cache[base + v] = wgt;
@@ -211,6 +218,7 @@ k_mlem(const GridF g, const GeometryDev geo, const float* __restrict__ sens,
         load_pixels(g, geo, sens, f, md, R, c0, n_pix, lane, sm.px);
       }
       int j = j0, pz = pz0;
+#pragma unroll kUnroll
       for (int v = lane; v < nv; v += 32) {
         const int iz = f.plane_begin + pz;
         const int vi = sm.px.base[j] + iz;
@@ -218,8 +226,8 @@ k_mlem(const GridF g, const GeometryDev geo, const float* __restrict__ sens,
         if (base + v < kCache) {
           wgt = sm.cache[base + v];
         } else {
-          wgt = voxel_kw(g, f, sm.px, j, iz, half_L);
-          if (wgt != 0.0f) wgt *= __ldg(rho_t + vi);
+          const float rho = __ldg(rho_t + vi);
+          wgt = voxel_kw(g, f, sm.px, j, iz, half_L) * rho;
         }
         if (wgt != 0.0f) atomicAdd(acc_t + vi, wgt * inv);
         j += q;
