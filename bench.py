@@ -543,6 +543,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-differentiable", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--path", default="strip", choices=["strip", "hybrid"],
+                    help="strip: the 2D strip MLEM headline; hybrid: the 3D hybrid MLEM")
+    ap.add_argument("--hybrid-events", type=int, default=10_000_000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", 0))
@@ -550,6 +553,13 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if world > 1 and "RANK" not in os.environ:
         sys.exit("for --gpus N > 1 launch under torchrun (one rank per GPU)")
+    if args.path == "hybrid":
+        import bench_hybrid
+        if args.e2e_iters == 20:
+            args.e2e_iters = 10
+        if args.impl == "reference":
+            return bench_hybrid.reference_arm(args, rank, world, host_cores())
+        return bench_hybrid.ours(args, rank, world, local_rank, ClockSampler, host_cores)
     if args.impl == "reference":
         return reference_arm(args, rank, world)
     return ours(args, rank, world, local_rank)

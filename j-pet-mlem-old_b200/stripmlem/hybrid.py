@@ -400,3 +400,104 @@ class HybridReconstruction:
             self._ctx, _vp(out["lor"]), _vp(out["info_begin"]), _vp(out["info_end"]),
             _vp(out["plane_begin"]), _vp(out["plane_end"]), _vp(out["index"])))
         return out
+
+
+# --- GATE text converters (3d_tool_convert) ---------------------------------------
+
+_CM = 0.01
+_C_PS = 299792458.0e-12          # speed of light, m / ps
+_C_SCINT_PS = 126000000.0e-12    # signal speed in the scintillator, m / ps
+
+
+def _contains(polygons, x, y, tol):
+    """Polygon::contains(p, tol) (src/2d/geometry/polygon.h:70-83) of every
+    point against every detector, binary32 as the reference: -> (n, n_det)."""
+    poly = np.asarray(polygons, np.float32)
+    px = np.asarray(x, np.float32)[:, None]
+    py = np.asarray(y, np.float32)[:, None]
+    inside = np.ones((len(px), len(poly)), bool)
+    start = poly[:, -1, :]
+    for i in range(poly.shape[1]):
+        end = poly[:, i, :]
+        ex, ey = end[:, 0] - start[:, 0], end[:, 1] - start[:, 1]
+        # cw_perpendicular (ey, -ex) . (p - start)
+        d = ey[None, :] * (px - start[None, :, 0]) + (-ex)[None, :] * (py - start[None, :, 1])
+        inside &= ~(d < np.float32(-tol))
+        start = end
+    return inside
+
+
+def convert_warsaw(lines, polygons, length, sigma_z=0.0, sigma_dl=0.0, seed=0, only=0,
+                   chunk=65536):
+    """3d_tool_convert --warsaw (src/3d/tool/convert_cmd.cpp:86-162): GATE
+    hit pairs `x1 y1 z1 t1 x2 y2 z2 t2 ... scatter` (cm, ps; the column count
+    from the first line, scatter the last column) -> responses (first,
+    second, z_up, z_dn, dl) in metres, binary64 as the reference prints them.
+    Pairs with |z| > length / 2 are skipped, as are pairs whose scatter
+    differs from `only` (when only != 0) and points inside no detector
+    (Polygon::contains with tolerance 1e-4); the larger detector index comes
+    first.  With sigma_z = sigma_dl = 0 the output is the reference's exactly;
+    otherwise the Gaussian errors come from numpy's generator, not the
+    reference's std::mt19937_64."""
+    rows = [ln.split() for ln in lines if ln.strip()]
+    if not rows:
+        z = np.zeros(0)
+        return np.zeros(0, np.int16), np.zeros(0, np.int16), z, z, z
+    n_col = len(rows[0])
+    a = np.array([[float(v) for v in r[:8]] + [float(r[n_col - 1])] for r in rows])
+    x1, y1, z1, t1, x2, y2, z2, t2, sc = a.T
+    keep = ~((np.abs(z1 * _CM) > length / 2) | (np.abs(z2 * _CM) > length / 2))
+    if only:
+        keep &= sc.astype(np.int64) == only
+    idx = np.flatnonzero(keep)
+    d1 = np.full(len(a), -1, np.int64)
+    d2 = np.full(len(a), -1, np.int64)
+    n_det = len(polygons)
+    for s in range(0, len(idx), chunk):
+        k = idx[s:s + chunk]
+        for pts, dd in (((x1, y1), d1), ((x2, y2), d2)):
+            inside = _contains(polygons, pts[0][k] * _CM, pts[1][k] * _CM, 0.0001)
+            last = n_det - 1 - np.argmax(inside[:, ::-1], axis=1)  # the last detector wins
+            dd[k] = np.where(inside.any(1), last, -1)
+    ok = keep & (d1 >= 0) & (d2 >= 0)
+    d1, d2, z1, z2, t1, t2 = d1[ok], d2[ok], z1[ok], z2[ok], t1[ok], t2[ok]
+    sw = d1 < d2
+    d1, d2 = np.where(sw, d2, d1), np.where(sw, d1, d2)
+    z1, z2 = np.where(sw, z2, z1), np.where(sw, z1, z2)
+    t1, t2 = np.where(sw, t2, t1), np.where(sw, t1, t2)
+    dl = (t1 - t2) * _C_PS
+    rng = np.random.default_rng(seed)
+    n = len(d1)
+    ez1 = rng.normal(0, sigma_z, n) if sigma_z > 0 else 0.0
+    ez2 = rng.normal(0, sigma_z, n) if sigma_z > 0 else 0.0
+    edl = rng.normal(0, sigma_dl, n) if sigma_dl > 0 else 0.0
+    return (d1.astype(np.int16), d2.astype(np.int16), z1 * _CM + ez1, z2 * _CM + ez2, dl + edl)
+
+
+def convert_tbednarski(lines, relative_time=False):
+    """3d_tool_convert --tbednarski (convert_cmd.cpp:164-211): records
+    `du dd t_ul t_ur t_dl t_dr` (detectors from 1, times in ps).  Default:
+    responses (first, second, z_up, z_dn, dl) with the larger detector first
+    (its times swapped along), indices from 0, z = c_scint (t_l - t_r) / 2,
+    dl = c ((t_ul + t_ur) - (t_dl + t_dr)) / 2.  relative_time: the records
+    with every time less the record's smallest, detectors unchanged."""
+    rows = [ln.split() for ln in lines if ln.strip()]
+    if not rows:
+        z = np.zeros(0)
+        return (np.zeros(0, np.int64),) * 2 + (z,) * 4 if relative_time else \
+            (np.zeros(0, np.int16),) * 2 + (z,) * 3
+    du = np.array([int(r[0]) for r in rows])
+    dd = np.array([int(r[1]) for r in rows])
+    t = np.array([[float(v) for v in r[2:6]] for r in rows])
+    tul, tur, tdl, tdr = t.T
+    if relative_time:
+        tmin = np.minimum(np.minimum(tur, tul), np.minimum(tdr, tdl))
+        return du, dd, tul - tmin, tur - tmin, tdl - tmin, tdr - tmin
+    sw = du < dd
+    du, dd = np.where(sw, dd, du), np.where(sw, du, dd)
+    tul, tdl = np.where(sw, tdl, tul), np.where(sw, tul, tdl)
+    tur, tdr = np.where(sw, tdr, tur), np.where(sw, tur, tdr)
+    zu = 0.5 * _C_SCINT_PS * (tul - tur)
+    zd = 0.5 * _C_SCINT_PS * (tdl - tdr)
+    dl = 0.5 * _C_PS * ((tul + tur) - (tdl + tdr))
+    return (du - 1).astype(np.int16), (dd - 1).astype(np.int16), zu, zd, dl
