@@ -74,7 +74,9 @@ typedef struct hybrid_stats {
 enum hybrid_sensitivity_mode {
   HYBRID_SENS_CALCULATE = 0, /* calculate_sensitivity: sum of LOR weights   */
   HYBRID_SENS_ONE = 1,       /* --sens-to-one                               */
-  HYBRID_SENS_EXTERNAL = 2   /* --sensitivity: caller's 2D map              */
+  HYBRID_SENS_EXTERNAL = 2,  /* --sensitivity: caller's 2D map              */
+  HYBRID_SENS_GIVEN = 3      /* caller's 2D map, weights already normalised
+                                (the GPU run()'s inputs)                    */
 };
 
 typedef void (*hybrid_progress_cb)(int32_t iteration, int32_t finished, void* user);
@@ -103,6 +105,18 @@ int hybrid_set_geometry_from_matrix(hybrid_ctx* ctx, int32_t n_detectors,
                                     const uint32_t* hits, uint32_t n_emissions,
                                     const int16_t* inactive, int32_t n_inactive);
 
+/* Takes a flattened geometry as the reference's GPU entry point receives it
+ * (GeometrySOA, src/2d/barrel/geometry_soa.h:270-284): per LOR index
+ * first * (first + 1) / 2 + second its segment (start x, y, end x, y; the
+ * mid point, direction and length are derived as LineSegment's constructor
+ * does, line_segment.h:18-27) and [lor_begin, lor_end) into the pixel-info
+ * arrays; per pixel info its pixel (x, y), position along the LOR and
+ * weight.  Use HYBRID_SENS_GIVEN when the weights are normalised already. */
+int hybrid_set_geometry_soa(hybrid_ctx* ctx, int32_t n_detectors, const float* segments,
+                            int64_t n_infos, const int16_t* pixels, const float* positions,
+                            const float* weights, const uint64_t* lor_begin,
+                            const uint64_t* lor_end);
+
 /* Copies the flattened geometry back (sizes from hybrid_get_stats):
  * seg 9 floats per LOR (start xy, end xy, mid xy, direction xy, length),
  * pix 2 int16 per info, pos / weight per info (weights as normalised by
@@ -129,6 +143,16 @@ int hybrid_get_sensitivity(hybrid_ctx* ctx, float* sens /* n_columns*n_rows */);
 int hybrid_set_responses(hybrid_ctx* ctx, const int16_t* first, const int16_t* second,
                          const float* z_up, const float* z_dn, const float* dl,
                          int64_t n);
+
+/* Takes frame events as the reference's GPU entry point receives them
+ * (Reconstruction::FrameEvent, reconstruction.h:53-63: the LOR's index,
+ * [pixel_info_begin, pixel_info_end), [plane_begin, plane_end), up, right,
+ * tan, sec), already translated and filtered by the caller.  Replaces the
+ * previous responses or frames. */
+int hybrid_set_frames(hybrid_ctx* ctx, int64_t n, const int32_t* lor, const int64_t* info_begin,
+                      const int64_t* info_end, const int16_t* plane_begin,
+                      const int16_t* plane_end, const float* up, const float* right,
+                      const float* tan, const float* sec);
 
 /* Frame events of kept responses in input order, for parity checks:
  * per event its LOR index, [info_begin, info_end), [plane_begin,

@@ -161,6 +161,48 @@ void free_geometry(hybrid_ctx* ctx) {
   ctx->have_sens = false;
 }
 
+// Uploads a flattened geometry (host arrays in GeometrySOA order) and
+// resets the sensitivity, events and statistics.
+int upload_geometry(hybrid_ctx* ctx, int32_t n_detectors, std::vector<float>& seg,
+                    const std::vector<int64_t>& lbeg, const std::vector<int64_t>& lend,
+                    const std::vector<int16_t>& pix, const std::vector<float>& pos,
+                    const std::vector<float>& w, int64_t n_infos) {
+  const int64_t n_lors = (int64_t)lbeg.size();
+  free_geometry(ctx);
+  std::vector<float4> md(n_lors);
+  std::vector<float> len(n_lors);
+  for (int64_t li = 0; li < n_lors; ++li) {
+    const float* sg = seg.data() + li * 9;
+    md[li] = make_float4(sg[4], sg[5], sg[6], sg[7]);
+    len[li] = sg[8];
+  }
+  CK(cudaMalloc(&ctx->d_md, n_lors * sizeof(float4)));
+  CK(cudaMalloc(&ctx->d_len, n_lors * sizeof(float)));
+  CK(cudaMalloc(&ctx->d_lbeg, n_lors * sizeof(int64_t)));
+  CK(cudaMalloc(&ctx->d_lend, n_lors * sizeof(int64_t)));
+  CK(cudaMalloc(&ctx->d_pix, n_infos * sizeof(short2)));
+  CK(cudaMalloc(&ctx->d_pos, n_infos * sizeof(float)));
+  CK(cudaMalloc(&ctx->d_w_raw, n_infos * sizeof(float)));
+  CK(cudaMalloc(&ctx->d_w, n_infos * sizeof(float)));
+  CK(cudaMemcpyAsync(ctx->d_md, md.data(), n_lors * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_len, len.data(), n_lors * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_lbeg, lbeg.data(), n_lors * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_lend, lend.data(), n_lors * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_pix, pix.data(), n_infos * sizeof(short2), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_pos, pos.data(), n_infos * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_w_raw, w.data(), n_infos * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_w, w.data(), n_infos * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->seg.swap(seg);
+  ctx->n_detectors = n_detectors;
+  ctx->n_lors = n_lors;
+  ctx->n_infos = n_infos;
+  ctx->stats = hybrid_stats{};
+  ctx->stats.n_lors = n_lors;
+  ctx->stats.n_pixel_infos = n_infos;
+  return STRIP_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -341,39 +383,38 @@ int hybrid_set_geometry_from_matrix(hybrid_ctx* ctx, int32_t n_detectors,
       std::copy(spos.begin(), spos.end(), pos.begin() + b);
     }
   }
-  free_geometry(ctx);
-  std::vector<float4> md(n_lors);
-  std::vector<float> len(n_lors);
+  return upload_geometry(ctx, n_detectors, seg, lbeg, lend, pix, pos, w, n_infos);
+}
+
+int hybrid_set_geometry_soa(hybrid_ctx* ctx, int32_t n_detectors, const float* segments,
+                            int64_t n_infos, const int16_t* pixels, const float* positions,
+                            const float* weights, const uint64_t* lor_begin,
+                            const uint64_t* lor_end) {
+  if (!ctx) return STRIP_E_INVALID;
+  if (n_detectors <= 0 || n_detectors > 32767 || !segments || n_infos <= 0 ||
+      n_infos >= ((int64_t)1 << 31) || !pixels || !positions || !weights || !lor_begin ||
+      !lor_end)
+    return fail(ctx, STRIP_E_INVALID, "invalid geometry arguments");
+  CK(cudaSetDevice(ctx->device));
+  const int64_t n_lors = lor_index(n_detectors, 0);
+  std::vector<float> seg(n_lors * 9);
+  std::vector<int64_t> lbeg(n_lors), lend(n_lors);
   for (int64_t li = 0; li < n_lors; ++li) {
-    const float* sg = seg.data() + li * 9;
-    md[li] = make_float4(sg[4], sg[5], sg[6], sg[7]);
-    len[li] = sg[8];
+    const float* s4 = segments + 4 * li;
+    make_segment(s4[0], s4[1], s4[2], s4[3], seg.data() + 9 * li);
+    if (lor_begin[li] > lor_end[li] || lor_end[li] > (uint64_t)n_infos)
+      return fail(ctx, STRIP_E_INVALID, "LOR %lld: pixel-info range out of bounds",
+                  (long long)li);
+    lbeg[li] = (int64_t)lor_begin[li];
+    lend[li] = (int64_t)lor_end[li];
   }
-  CK(cudaMalloc(&ctx->d_md, n_lors * sizeof(float4)));
-  CK(cudaMalloc(&ctx->d_len, n_lors * sizeof(float)));
-  CK(cudaMalloc(&ctx->d_lbeg, n_lors * sizeof(int64_t)));
-  CK(cudaMalloc(&ctx->d_lend, n_lors * sizeof(int64_t)));
-  CK(cudaMalloc(&ctx->d_pix, n_infos * sizeof(short2)));
-  CK(cudaMalloc(&ctx->d_pos, n_infos * sizeof(float)));
-  CK(cudaMalloc(&ctx->d_w_raw, n_infos * sizeof(float)));
-  CK(cudaMalloc(&ctx->d_w, n_infos * sizeof(float)));
-  CK(cudaMemcpyAsync(ctx->d_md, md.data(), n_lors * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemcpyAsync(ctx->d_len, len.data(), n_lors * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemcpyAsync(ctx->d_lbeg, lbeg.data(), n_lors * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemcpyAsync(ctx->d_lend, lend.data(), n_lors * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemcpyAsync(ctx->d_pix, pix.data(), n_infos * sizeof(short2), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemcpyAsync(ctx->d_pos, pos.data(), n_infos * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemcpyAsync(ctx->d_w_raw, w.data(), n_infos * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemcpyAsync(ctx->d_w, w.data(), n_infos * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  ctx->seg.swap(seg);
-  ctx->n_detectors = n_detectors;
-  ctx->n_lors = n_lors;
-  ctx->n_infos = n_infos;
-  ctx->stats = hybrid_stats{};
-  ctx->stats.n_lors = n_lors;
-  ctx->stats.n_pixel_infos = n_infos;
-  return STRIP_OK;
+  std::vector<int16_t> pix(pixels, pixels + 2 * n_infos);
+  for (int64_t i = 0; i < n_infos; ++i)
+    if (pix[2 * i] < 0 || pix[2 * i] >= ctx->setup.n_columns || pix[2 * i + 1] < 0 ||
+        pix[2 * i + 1] >= ctx->setup.n_rows)
+      return fail(ctx, STRIP_E_INVALID, "pixel info %lld: pixel out of range", (long long)i);
+  std::vector<float> pos(positions, positions + n_infos), w(weights, weights + n_infos);
+  return upload_geometry(ctx, n_detectors, seg, lbeg, lend, pix, pos, w, n_infos);
 }
 
 int hybrid_get_geometry(hybrid_ctx* ctx, float* seg, int16_t* pix, float* pos, float* weight,
@@ -395,9 +436,10 @@ int hybrid_get_geometry(hybrid_ctx* ctx, float* seg, int16_t* pix, float* pos, f
 int hybrid_set_sensitivity(hybrid_ctx* ctx, int32_t mode, const float* external) {
   if (!ctx) return STRIP_E_INVALID;
   if (!ctx->n_lors) return fail(ctx, STRIP_E_STATE, "set the geometry first");
-  if (mode != HYBRID_SENS_CALCULATE && mode != HYBRID_SENS_ONE && mode != HYBRID_SENS_EXTERNAL)
+  if (mode != HYBRID_SENS_CALCULATE && mode != HYBRID_SENS_ONE &&
+      mode != HYBRID_SENS_EXTERNAL && mode != HYBRID_SENS_GIVEN)
     return fail(ctx, STRIP_E_INVALID, "unknown sensitivity mode %d", mode);
-  if (mode == HYBRID_SENS_EXTERNAL && !external)
+  if ((mode == HYBRID_SENS_EXTERNAL || mode == HYBRID_SENS_GIVEN) && !external)
     return fail(ctx, STRIP_E_INVALID, "external sensitivity map is null");
   CK(cudaSetDevice(ctx->device));
   const GridF& g = ctx->g;
@@ -406,14 +448,15 @@ int hybrid_set_sensitivity(hybrid_ctx* ctx, int32_t mode, const float* external)
                        ctx->stream);
   } else {
     std::vector<float> h(g.n_pixels, 1.0f);
-    if (mode == HYBRID_SENS_EXTERNAL) std::copy(external, external + g.n_pixels, h.begin());
+    if (mode != HYBRID_SENS_ONE) std::copy(external, external + g.n_pixels, h.begin());
     CK(cudaMemcpyAsync(ctx->d_sens, h.data(), g.n_pixels * sizeof(float), cudaMemcpyHostToDevice,
                        ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
   }
   CK(cudaMemcpyAsync(ctx->d_w, ctx->d_w_raw, ctx->n_infos * sizeof(float),
                      cudaMemcpyDeviceToDevice, ctx->stream));
-  launch_normalize(g, ctx->d_pix, ctx->d_w, ctx->d_sens, ctx->n_infos, ctx->stream);
+  if (mode != HYBRID_SENS_GIVEN)  // GIVEN: the weights are normalised already
+    launch_normalize(g, ctx->d_pix, ctx->d_w, ctx->d_sens, ctx->n_infos, ctx->stream);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(ctx->stream));
   free_events(ctx);  // frame events depend on the normalised weights
@@ -515,6 +558,58 @@ int hybrid_set_responses(hybrid_ctx* ctx, const int16_t* first, const int16_t* s
   cleanup();
   ctx->n_events = kept;
   ctx->stats.n_events = kept;
+  return STRIP_OK;
+}
+
+int hybrid_set_frames(hybrid_ctx* ctx, int64_t n, const int32_t* lor, const int64_t* info_begin,
+                      const int64_t* info_end, const int16_t* plane_begin,
+                      const int16_t* plane_end, const float* up, const float* right,
+                      const float* tan, const float* sec) {
+  if (!ctx) return STRIP_E_INVALID;
+  if (n < 0 || (n > 0 && (!lor || !info_begin || !info_end || !plane_begin || !plane_end ||
+                          !up || !right || !tan || !sec)))
+    return fail(ctx, STRIP_E_INVALID, "invalid frame events");
+  if (!ctx->n_lors) return fail(ctx, STRIP_E_STATE, "set the geometry first");
+  CK(cudaSetDevice(ctx->device));
+  std::vector<Frame> h(n);
+  std::vector<int64_t> index(n);
+  for (int64_t i = 0; i < n; ++i) {
+    if (lor[i] < 0 || lor[i] >= ctx->n_lors || info_begin[i] < 0 ||
+        info_end[i] > ctx->n_infos || plane_begin[i] < 0 || plane_end[i] > ctx->g.np)
+      return fail(ctx, STRIP_E_INVALID, "frame event %lld out of range", (long long)i);
+    Frame& f = h[i];
+    f.lor = lor[i];
+    f.info_begin = (int32_t)info_begin[i];
+    f.info_end = (int32_t)info_end[i];
+    f.plane_begin = plane_begin[i];
+    f.plane_end = plane_end[i];
+    f.up = up[i];
+    f.right = right[i];
+    f.tan = tan[i];
+    f.sec = sec[i];
+    index[i] = i;
+  }
+  free_events(ctx);
+  ctx->n_responses = n;
+  ctx->stats.n_responses = n;
+  ctx->stats.n_events = 0;
+  ctx->stats.used_pixels = ctx->stats.used_voxels = 0;
+  if (n == 0) return STRIP_OK;
+  CK(cudaMalloc(&ctx->d_frames, n * sizeof(Frame)));
+  CK(cudaMalloc(&ctx->d_index, n * sizeof(int64_t)));
+  CK(cudaMemcpyAsync(ctx->d_frames, h.data(), n * sizeof(Frame), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CK(cudaMemcpyAsync(ctx->d_index, index.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  launch_event_counts(ctx->d_frames, n, ctx->d_counts, ctx->stream);
+  CK(cudaGetLastError());
+  unsigned long long counts[2] = {0, 0};
+  CK(cudaMemcpyAsync(counts, ctx->d_counts, sizeof counts, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->stats.used_pixels = (int64_t)counts[0];
+  ctx->stats.used_voxels = (int64_t)counts[1];
+  ctx->n_events = n;
+  ctx->stats.n_events = n;
   return STRIP_OK;
 }
 

@@ -250,7 +250,7 @@ class HybridCylinder(ctypes.Structure):
                 ("x", "y", "z", "radius", "half_length", "activity")]
 
 
-HYBRID_SENS_CALCULATE, HYBRID_SENS_ONE, HYBRID_SENS_EXTERNAL = 0, 1, 2
+HYBRID_SENS_CALCULATE, HYBRID_SENS_ONE, HYBRID_SENS_EXTERNAL, HYBRID_SENS_GIVEN = 0, 1, 2, 3
 HYBRID_PROGRESS_CB = ctypes.CFUNCTYPE(None, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p)
 _vp = ctypes.c_void_p
 
@@ -264,6 +264,9 @@ SIGNATURES.update({
         [_ctx, ctypes.c_int32, _vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp, ctypes.c_uint32,
          _vp, ctypes.c_int32]),
     "hybrid_get_geometry": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "hybrid_set_geometry_soa": (
+        ctypes.c_int, [_ctx, ctypes.c_int32, _vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp]),
+    "hybrid_set_frames": (ctypes.c_int, [_ctx, ctypes.c_int64] + [_vp] * 9),
     "hybrid_set_sensitivity": (ctypes.c_int, [_ctx, ctypes.c_int32, _vp]),
     "hybrid_get_sensitivity": (ctypes.c_int, [_ctx, _vp]),
     "hybrid_set_responses": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp, _vp, ctypes.c_int64]),

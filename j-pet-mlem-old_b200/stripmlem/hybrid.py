@@ -330,7 +330,37 @@ class HybridReconstruction:
             _vp(matrix.px), _vp(matrix.py), _vp(matrix.hits), matrix.n_emissions, _vp(ina),
             0 if ina is None else len(ina)))
 
-    def set_sensitivity(self, sensitivity="calculate"):
+    def set_geometry_soa(self, n_detectors, segments, pixels, positions, weights, lor_begin,
+                         lor_end):
+        """A flattened geometry as the reference's GPU run() receives it:
+        segments (n_lors, 4) start / end points, pixels (n, 2), positions,
+        weights, per-LOR [lor_begin, lor_end)."""
+        seg = np.ascontiguousarray(segments, np.float32).reshape(-1, 4)
+        pix = np.ascontiguousarray(pixels, np.int16).reshape(-1, 2)
+        pos = np.ascontiguousarray(positions, np.float32)
+        w = np.ascontiguousarray(weights, np.float32)
+        lb = np.ascontiguousarray(lor_begin, np.uint64)
+        le = np.ascontiguousarray(lor_end, np.uint64)
+        self._check(self.lib.hybrid_set_geometry_soa(self._ctx, n_detectors, _vp(seg), len(pos),
+                                                     _vp(pix), _vp(pos), _vp(w), _vp(lb),
+                                                     _vp(le)))
+
+    def set_frames(self, lor, info_begin, info_end, plane_begin, plane_end, up, right, tan, sec):
+        """Frame events as the reference's GPU run() receives them."""
+        a = [np.ascontiguousarray(x, t) for x, t in (
+            (lor, np.int32), (info_begin, np.int64), (info_end, np.int64),
+            (plane_begin, np.int16), (plane_end, np.int16), (up, np.float32),
+            (right, np.float32), (tan, np.float32), (sec, np.float32))]
+        self._check(self.lib.hybrid_set_frames(self._ctx, len(a[0]), *[_vp(x) for x in a]))
+
+    def set_sensitivity(self, sensitivity="calculate", given=False):
+        """'calculate', 'one' or a 2D map; with given=True the map is used as
+        is and the weights are taken as normalised already."""
+        if given:
+            s = np.ascontiguousarray(sensitivity, np.float32).reshape(-1)
+            self._check(self.lib.hybrid_set_sensitivity(self._ctx, _lib.HYBRID_SENS_GIVEN,
+                                                        _vp(s)))
+            return
         if isinstance(sensitivity, str):
             mode = {"calculate": _lib.HYBRID_SENS_CALCULATE, "one": _lib.HYBRID_SENS_ONE}[sensitivity]
             self._check(self.lib.hybrid_set_sensitivity(self._ctx, mode, None))

@@ -176,3 +176,29 @@ def test_device_generator_equals_host_generator():
     for a, c in zip(h[2:], d[2:]):
         assert np.allclose(a[same], c[same], rtol=0, atol=1e-5)
 
+
+
+def test_geometry_soa_and_frames_entry_points():
+    """The GPU run()'s inputs: the oracle's flattened geometry with its
+    normalised weights and sensitivity (HYBRID_SENS_GIVEN) and its frame
+    events reproduce the reference's image."""
+    from oracle import hybrid as oh
+    from stripmlem import hybrid as hy
+    z, cfg, m, resp, centers = golden_inputs()
+    n, n_planes, p, z_left, length, s_z, s_dl = cfg
+    s = oracle_setup(cfg)
+    ora = oh.reconstruct(s, centers, m, resp, 0)
+    geo, fr = ora["geo"], ora["frames"]
+    with hy.HybridReconstruction(n, n, n_planes, p, z_left, length, s_z, s_dl) as rec:
+        rec.set_geometry_soa(len(centers), geo["seg"][:, :4], geo["pix"], geo["pos"], ora["w"],
+                             geo["lbeg"], geo["lend"])
+        rec.set_sensitivity(ora["sens"], given=True)
+        g = rec.geometry()
+        assert np.array_equal(g["seg"], geo["seg"], equal_nan=True)
+        assert np.array_equal(g["w"], ora["w"])
+        rec.set_frames(fr["lor_index"], fr["info_begin"], fr["info_end"], fr["plane_begin"],
+                       fr["plane_end"], fr["up"], fr["right"], fr["tan"], fr["sec"])
+        assert rec.stats()["used_voxels"] == int(z["calc_counts"][2])
+        rec(3)
+        img = rec.rho
+    assert rel_l2(img, z["calc_rho"]) < TOL
