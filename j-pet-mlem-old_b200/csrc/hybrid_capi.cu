@@ -52,6 +52,7 @@ struct hybrid_ctx {
   float* d_rho_t = nullptr;
   float* d_acc_t = nullptr;
   float* d_tmp = nullptr;  // boundary-layout staging
+  float* d_spill = nullptr;  // per-warp weight slabs of k_mlem
   hybrid_stats stats{};
   std::string err;
 };
@@ -274,6 +275,7 @@ int hybrid_ctx_destroy(hybrid_ctx* ctx) {
   dfree(ctx->d_rho_t);
   dfree(ctx->d_acc_t);
   dfree(ctx->d_tmp);
+  dfree(ctx->d_spill);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -643,13 +645,14 @@ int hybrid_iterate(hybrid_ctx* ctx, int32_t n_iterations, hybrid_progress_cb pro
   CK(cudaSetDevice(ctx->device));
   const size_t vb = ctx->n_voxels * sizeof(float);
   const int blocks = ctx->sm_count * mlem_blocks_per_sm();
+  if (!ctx->d_spill) CK(cudaMalloc(&ctx->d_spill, mlem_spill_floats(blocks) * sizeof(float)));
   for (int32_t it = 0; it < n_iterations; ++it) {
     if (progress) progress(ctx->stats.iterations, 0, user);
     CK(cudaMemsetAsync(ctx->d_acc_t, 0, vb, ctx->stream));
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     if (ctx->n_events > 0)
       launch_mlem(ctx->g, geo_view(ctx), ctx->d_sens, ctx->d_frames, ctx->n_events, ctx->d_rho_t,
-                  ctx->d_acc_t, blocks, ctx->stream);
+                  ctx->d_acc_t, ctx->d_spill, blocks, ctx->stream);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
     CK(cudaEventSynchronize(ctx->ev1));

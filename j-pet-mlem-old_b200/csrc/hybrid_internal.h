@@ -69,9 +69,12 @@ void launch_compact(const Frame* frames, const int32_t* keep, const int64_t* off
 // hybrid_kernels.cu
 void launch_to_zfast(const GridF& g, const float* rho, float* rho_t, cudaStream_t st);
 void launch_from_zfast(const GridF& g, const float* rho_t, float* rho, cudaStream_t st);
+// spill: mlem_spill_floats(n_blocks) floats of scratch for the per-warp
+// weight slabs.
 void launch_mlem(const GridF& g, const GeometryDev& geo, const float* sens, const Frame* frames,
-                 int64_t n_frames, const float* rho_t, float* acc_t, int n_blocks,
+                 int64_t n_frames, const float* rho_t, float* acc_t, float* spill, int n_blocks,
                  cudaStream_t st);
+size_t mlem_spill_floats(int n_blocks);
 int mlem_blocks_per_sm();
 void launch_event_counts(const Frame* frames, int64_t n, unsigned long long* out2,
                          cudaStream_t st);

@@ -22,7 +22,9 @@
 // 1 / sens per pixel info and plane -- it depends on the LOR, the pixel and
 // the plane only -- was slower: 414 against 252 ms per iteration on the
 // big-barrel workload, the walk waiting on its HBM loads.)  Pass 1 keeps each
-// voxel's weight in a per-warp shared cache (first kCache voxels); pass 2
+// voxel's weight in a per-warp shared cache (first kCache voxels) and the
+// next kSpill in a per-warp slab of global memory (written and read back by
+// the same warp within microseconds, so it stays in L2); pass 2
 // scatters weight / D with one red.global.add.f32 per voxel, reading the
 // cache or recomputing past it.
 #include "hybrid_internal.h"
@@ -41,12 +43,16 @@ namespace {
 #ifndef HYBRID_BLOCKS_PER_SM
 #define HYBRID_BLOCKS_PER_SM 3
 #endif
+#ifndef HYBRID_SPILL
+#define HYBRID_SPILL 16384
+#endif
 #ifndef HYBRID_UNROLL
 #define HYBRID_UNROLL 1
 #endif
 constexpr int kWarps = HYBRID_WARPS;
 constexpr int kThreads = kWarps * 32;
 constexpr int kCache = HYBRID_CACHE;          // cached voxel weights per warp
+constexpr int kSpill = HYBRID_SPILL;          // further weights per warp in global memory
 constexpr int kBlocksPerSm = HYBRID_BLOCKS_PER_SM;
 constexpr int kUnroll = HYBRID_UNROLL;           // voxel-loop unroll
 
@@ -156,11 +162,12 @@ __device__ __forceinline__ float voxel_kw(const GridF& g, const Frame& f, const 
 __global__ void __launch_bounds__(kThreads, kBlocksPerSm)
 k_mlem(const GridF g, const GeometryDev geo, const float* __restrict__ sens,
        const Frame* __restrict__ frames, int64_t n_frames,
-       const float* __restrict__ rho_t, float* acc_t) {
+       const float* __restrict__ rho_t, float* acc_t, float* spill) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   WarpSmem& sm = reinterpret_cast<WarpSmem*>(smem_raw)[wib];
+  float* slab = spill + ((int64_t)blockIdx.x * kWarps + wib) * kSpill;
   const int64_t n_warps = (int64_t)gridDim.x * kWarps;
   const float half_L = g.L / 2;
   for (int64_t e = (int64_t)blockIdx.x * kWarps + wib; e < n_frames; e += n_warps) {
@@ -189,7 +196,11 @@ k_mlem(const GridF g, const GeometryDev geo, const float* __restrict__ sens,
           wgt *= rho;
           d = fmaf(wgt, sm.px.t[j].w, d);
         }
-        if (base + v < kCache) sm.cache[base + v] = wgt;
+        const int fv = base + v;
+        if (fv < kCache)
+          sm.cache[fv] = wgt;
+        else if (fv < kCache + kSpill)
+          slab[fv - kCache] = wgt;
         j += q;
         pz += r;
         if (pz >= n_pl) {
@@ -208,7 +219,7 @@ k_mlem(const GridF g, const GeometryDev geo, const float* __restrict__ sens,
     for (int c0 = 0; c0 < n_pix; c0 += 32) {
       const int base = c0 * n_pl;
       const int nv = min(32, n_pix - c0) * n_pl;
-      if (base + nv <= kCache) {
+      if (base + nv <= kCache + kSpill) {
         if (c0 + lane < n_pix) {
           const short2 p = geo.pix[(int64_t)f.info_begin + c0 + lane];
           sm.px.base[lane] = (p.x + g.nc * p.y) * g.np;
@@ -222,9 +233,12 @@ k_mlem(const GridF g, const GeometryDev geo, const float* __restrict__ sens,
       for (int v = lane; v < nv; v += 32) {
         const int iz = f.plane_begin + pz;
         const int vi = sm.px.base[j] + iz;
+        const int fv = base + v;
         float wgt;
-        if (base + v < kCache) {
-          wgt = sm.cache[base + v];
+        if (fv < kCache) {
+          wgt = sm.cache[fv];
+        } else if (fv < kCache + kSpill) {
+          wgt = slab[fv - kCache];
         } else {
           const float rho = __ldg(rho_t + vi);
           wgt = voxel_kw(g, f, sm.px, j, iz, half_L) * rho;
@@ -299,12 +313,14 @@ void launch_from_zfast(const GridF& g, const float* rho_t, float* rho, cudaStrea
   k_from_zfast<<<grid_for((int64_t)g.n_pixels * g.np), 256, 0, st>>>(g, rho_t, rho);
 }
 
+size_t mlem_spill_floats(int n_blocks) { return (size_t)n_blocks * kWarps * kSpill; }
+
 void launch_mlem(const GridF& g, const GeometryDev& geo, const float* sens, const Frame* frames,
-                 int64_t n_frames, const float* rho_t, float* acc_t, int n_blocks,
+                 int64_t n_frames, const float* rho_t, float* acc_t, float* spill, int n_blocks,
                  cudaStream_t st) {
   const int smem = (int)sizeof(WarpSmem) * kWarps;
   cudaFuncSetAttribute(k_mlem, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  k_mlem<<<n_blocks, kThreads, smem, st>>>(g, geo, sens, frames, n_frames, rho_t, acc_t);
+  k_mlem<<<n_blocks, kThreads, smem, st>>>(g, geo, sens, frames, n_frames, rho_t, acc_t, spill);
 }
 
 void launch_event_counts(const Frame* frames, int64_t n, unsigned long long* out2,
