@@ -49,12 +49,16 @@ namespace {
 #ifndef HYBRID_UNROLL
 #define HYBRID_UNROLL 1
 #endif
+#ifndef HYBRID_UNROLL2
+#define HYBRID_UNROLL2 1
+#endif
 constexpr int kWarps = HYBRID_WARPS;
 constexpr int kThreads = kWarps * 32;
 constexpr int kCache = HYBRID_CACHE;          // cached voxel weights per warp
 constexpr int kSpill = HYBRID_SPILL;          // further weights per warp in global memory
 constexpr int kBlocksPerSm = HYBRID_BLOCKS_PER_SM;
-constexpr int kUnroll = HYBRID_UNROLL;           // voxel-loop unroll
+constexpr int kUnroll = HYBRID_UNROLL;           // pass-1 voxel-loop unroll
+constexpr int kUnroll2 = HYBRID_UNROLL2;         // pass-2 voxel-loop unroll
 
 // atan2(a, b) for a > 0, in (0, pi): the quotient of the smaller by the
 // larger of a and |b| (fast division) folded into [0, 1], an odd polynomial
@@ -229,7 +233,7 @@ k_mlem(const GridF g, const GeometryDev geo, const float* __restrict__ sens,
         load_pixels(g, geo, sens, f, md, R, c0, n_pix, lane, sm.px);
       }
       int j = j0, pz = pz0;
-#pragma unroll kUnroll
+#pragma unroll kUnroll2
       for (int v = lane; v < nv; v += 32) {
         const int iz = f.plane_begin + pz;
         const int vi = sm.px.base[j] + iz;
