@@ -1,0 +1,178 @@
+"""Drop-in command line for the reference's 3d_hybrid_reconstruction
+(src/3d/hybrid/reconstruction_cmd.cpp:147-680, its --system matrix path) on
+the B200:
+
+    python -m stripmlem.hybrid_cli --system matrix_full.bin \\
+        --detector-file det.txt --detector-file-sym sym.txt -p 0.004 \\
+        --n-planes 125 --z-left -0.25 --length 0.5 -i 1 -I 10 -o rho.bin responses.bin
+
+Same flags, defaults and file formats as the reference: a full (PETP) system
+matrix; the detector description file (detector centres from its polygons);
+responses `first second z_up z_dn dl`, binary (16-byte records) or, for
+*.txt, text; --sens-to-one, --sensitivity (a 2D map, binary or *.txt),
+--inactive; --rho to start from an image; -i blocks x -I iterations.  With
+-o base.ext it writes, as the reference's CPU branch does, the naive image of
+the events' points `base.ext` (int32) and after each block
+`base_NN.ext` (binary32, or text for .txt), each with an NRRD header.
+Text responses are parsed with numpy (correctly rounded); the reference's
+fast text parser can differ from it in the last bit of a value.
+"""
+import argparse
+import os
+import sys
+
+import numpy as np
+
+from . import hybrid as hy
+
+
+def _ints(text):
+    return [int(v) for v in str(text).replace(",", " ").split()]
+
+
+def parse(argv=None):
+    ap = argparse.ArgumentParser(prog="3d_hybrid_reconstruction")
+    ap.add_argument("--system", "-s", required=True, help="system matrix file (full form)")
+    ap.add_argument("--detector-file", required=True, help="detector description file")
+    ap.add_argument("--detector-file-sym", default=None,
+                    help="detector symmetries description file (accepted, not used)")
+    ap.add_argument("--n-pixels", "-n", type=int, default=None)
+    ap.add_argument("--s-pixel", "-p", type=float, required=True)
+    ap.add_argument("--n-planes", type=int, default=None)
+    ap.add_argument("--z-left", type=float, default=None)
+    ap.add_argument("--length", "-l", type=float, default=2.0)
+    ap.add_argument("--s-z", type=float, default=0.015)
+    ap.add_argument("--s-dl", type=float, default=0.060)
+    ap.add_argument("--blocks", "-i", type=int, default=0)
+    ap.add_argument("--iterations", "-I", type=int, default=1)
+    ap.add_argument("--output", "-o", default=None)
+    ap.add_argument("--sens-to-one", action="store_true")
+    ap.add_argument("--sensitivity", default=None, help="external 2D sensitivity")
+    ap.add_argument("--inactive", default=None, help="list of inactive detectors")
+    ap.add_argument("--rho", default=None, help="start rho")
+    ap.add_argument("--cuda-device", "-D", type=int, default=0)
+    ap.add_argument("--verbose", "-v", action="count", default=0)
+    ap.add_argument("responses", nargs="*")
+    return ap.parse_args(argv)
+
+
+def _read_map(path, n):
+    if path.endswith(".txt"):
+        return np.loadtxt(path, dtype=np.float32).reshape(-1)[:n]
+    return np.fromfile(path, np.float32, n)
+
+
+def _write_map(base, ext, data, dims, kind):
+    fn = base + ext
+    if ext == ".txt":
+        with open(fn, "w") as f:
+            width = dims[0]
+            flat = data.reshape(-1)
+            for r in range(0, flat.size, width):
+                f.write(" ".join(("%d" if kind == "int" else "%g") % v
+                                 for v in flat[r:r + width]) + "\n")
+    else:
+        data.astype(np.int32 if kind == "int" else np.float32).tofile(fn)
+    with open(base + ".nrrd", "w") as f:
+        f.write("NRRD0001\ntype: %s\nendian: little\ndimension: 3\nsizes: %d %d %d\n"
+                "data file: ./%s\nencoding: %s\n"
+                % (kind, dims[0], dims[1], dims[2], os.path.basename(fn),
+                   "ascii" if ext == ".txt" else "raw"))
+
+
+def naive_image(kept, resp, n, n_planes, p, z_left, centers):
+    """Reconstruction::naive (reconstruction.h:394-405): the count of kept
+    events per voxel of their point (the LOR's mid point + up along it, z =
+    right), binary32 as the reference computes it.  kept: the kept responses'
+    indices."""
+    f32 = np.float32
+    idx = np.asarray(kept, np.int64)
+    first, second = resp[0][idx].astype(np.int64), resp[1][idx].astype(np.int64)
+    zu, zd, dl = (np.asarray(a, f32)[idx] for a in resp[2:])
+    cs, ce = centers[second].astype(f32), centers[first].astype(f32)
+    mid = (cs + ce) / f32(2)
+    v = ce - cs
+    ln = np.sqrt(v[:, 0] * v[:, 0] + v[:, 1] * v[:, 1])
+    d = v / ln[:, None]
+    R = ln / f32(2)
+    tan = (zu - zd) / (f32(2) * R)
+    up = f32(-0.5) * (dl / np.sqrt(f32(1) + tan * tan))
+    right = f32(0.5) * (zu + zd + (f32(2) * up * tan))
+    x = mid[:, 0] + d[:, 0] * up
+    y = mid[:, 1] + d[:, 1] * up
+    llx = -f32(p) * f32(n) / f32(2)
+    ix = np.floor((x - llx) / f32(p)).astype(np.int64)
+    iy = np.floor((y - llx) / f32(p)).astype(np.int64)
+    iz = np.floor((right - f32(z_left)) / f32(p)).astype(np.int64)
+    ok = (ix >= 0) & (ix < n) & (iy >= 0) & (iy < n) & (iz >= 0) & (iz < n_planes)
+    img = np.zeros((n_planes, n, n), np.int32)
+    np.add.at(img, (iz[ok], iy[ok], ix[ok]), 1)
+    return img
+
+
+def main(argv=None):
+    a = parse(argv)
+    m = hy.SystemMatrix.read(a.system)
+    n = a.n_pixels or m.n_pixels_in_row
+    n_planes = a.n_planes if a.n_planes is not None else n
+    z_left = a.z_left if a.z_left is not None else -n_planes * a.s_pixel / 2
+    polygons = hy.read_detector_file(a.detector_file)
+    if len(polygons) != m.n_detectors:
+        raise SystemExit("n_detectors mismatch")
+    centers = hy.detector_centers(polygons)
+    inactive = _ints(a.inactive) if a.inactive else None
+    if a.verbose:
+        print(f"3D hybrid reconstruction w/system matrix:\n    detectors = {m.n_detectors}",
+              file=sys.stderr)
+        print(f"   pixel grid = {n} x {n} / {a.s_pixel}", file=sys.stderr)
+    rec = hy.HybridReconstruction(n, n, n_planes, a.s_pixel, z_left, a.length, a.s_z, a.s_dl,
+                                  device=a.cuda_device)
+    rec.set_geometry_from_matrix(centers, m, inactive)
+    if a.sensitivity:
+        rec.set_sensitivity(_read_map(a.sensitivity, n * n))
+    elif a.sens_to_one:
+        rec.set_sensitivity("one")
+    else:
+        rec.set_sensitivity()
+    parts = [hy.read_responses(fn) for fn in a.responses]
+    resp = tuple(np.concatenate([p[k] for p in parts]) if parts else np.zeros(0)
+                 for k in range(5))
+    rec.set_responses(*resp)
+    st = rec.stats()
+    if a.verbose:
+        print(f"       events = {st['n_events']}", file=sys.stderr)
+    start = 0
+    if a.rho:
+        rec.rho = _read_map(a.rho, n * n * n_planes)
+        base = os.path.splitext(a.rho)[0]
+        digits = len(base) - len(base.rstrip("0123456789"))
+        start = int(base[len(base) - digits:]) if digits else 0
+    out_base, out_ext = os.path.splitext(a.output) if a.output else (None, None)
+    dims = (n, n, n_planes)
+    if out_base:
+        _write_map(out_base, out_ext, naive_image(rec.frames()["index"], resp, n, n_planes,
+                                                  a.s_pixel, z_left, centers), dims, "int")
+    n_total = a.blocks * a.iterations
+    digits = len(str(n_total)) if n_total > 0 else 1
+    for block in range(a.blocks):
+        first_it = block * a.iterations
+        todo = [i for i in range(first_it, first_it + a.iterations) if i >= start]
+        if todo:
+            rec(len(todo))
+        it = (block + 1) * a.iterations
+        if it <= start or not out_base:
+            continue
+        _write_map(f"{out_base}_{it:0{digits}d}", out_ext, rec.rho, dims, "float")
+    st = rec.stats()
+    print(f"  event count = {st['n_events']}", file=sys.stderr)
+    if st["n_events"]:
+        print(f"  voxel count = {st['used_voxels']}"
+              f"({st['used_voxels'] / st['n_events']:g} / event)", file=sys.stderr)
+        print(f"  pixel count = {st['used_pixels']}"
+              f"({st['used_pixels'] / st['n_events']:g} / event)", file=sys.stderr)
+    rec.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

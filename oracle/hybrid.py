@@ -183,5 +183,12 @@ def run_ref(workdir, matrix_path, detector_path, symmetry_path, responses_path, 
     return img.reshape(n_planes, n_pixels, n_pixels), p.stderr
 
 
+def ref_naive(workdir, n_pixels, n_planes):
+    """The naive image (event points counted per voxel, int32) that
+    run_ref's reference call wrote to rho.bin."""
+    return np.fromfile(os.path.join(workdir, "rho.bin"), np.int32).reshape(
+        n_planes, n_pixels, n_pixels)
+
+
 def tempdir():
     return tempfile.mkdtemp(prefix="hybref_")

@@ -12,7 +12,8 @@ of stripmlem.hybrid.synthetic_matrix on a 24 x 24 grid of 1 cm pixels, and
 seed 5) in a two-cylinder phantom; 24 planes, z_left -0.12 m, L 0.3 m,
 sigma_z 0.01 m, sigma_dl 0.04 m.  The npz holds the inputs (detector
 polygons, matrix elements, responses, setup) and, per case, the reference's
-image and its event / pixel / voxel counts:
+image, its naive image (event points per voxel) and its event / pixel / voxel
+counts:
   calc     calculate_sensitivity, 3 iterations
   one      --sens-to-one, 2 iterations
   inactive --inactive 3,40, 2 iterations
@@ -68,6 +69,7 @@ def main():
                               s["p"], s["n_planes"], s["z_left"], s["length"], s["sigma_z"],
                               s["sigma_dl"], n_iter, extra=extra)
         out[f"{name}_rho"] = img
+        out[f"{name}_naive"] = oh.ref_naive(d, s["n"], s["n_planes"])
         out[f"{name}_counts"] = counts(err)
         print(name, out[f"{name}_counts"], float(img.sum()))
     np.savez_compressed(os.path.join(HERE, "hybrid_small.npz"), **out)

@@ -202,3 +202,33 @@ def test_geometry_soa_and_frames_entry_points():
         rec(3)
         img = rec.rho
     assert rel_l2(img, z["calc_rho"]) < TOL
+
+
+@pytest.mark.parametrize("case,n_iter,extra", [("calc", 3, []), ("inactive", 2, ["--inactive", "3,40"]),
+                                               ("one", 2, ["--sens-to-one"])])
+def test_cli_drop_in(tmp_path, case, n_iter, extra):
+    """python -m stripmlem.hybrid_cli with the reference's flags on the
+    reference's file formats: the naive image bit for bit, the iterated image
+    within 1e-4 of the reference's own, the reference's output names."""
+    from stripmlem import hybrid as hy
+    from stripmlem import hybrid_cli
+    z, cfg, m, resp, centers = golden_inputs()
+    n, n_planes, p, z_left, length, s_z, s_dl = cfg
+    m.write(str(tmp_path / "m.bin"))
+    hy.write_detector_file(str(tmp_path / "det.txt"), z["polygons"])
+    hy.write_symmetry_file(str(tmp_path / "sym.txt"), len(z["polygons"]))
+    hy.write_responses(str(tmp_path / "r.bin"), *resp)
+    out = str(tmp_path / "rho.bin")
+    rc = hybrid_cli.main(["--system", str(tmp_path / "m.bin"),
+                          "--detector-file", str(tmp_path / "det.txt"),
+                          "--detector-file-sym", str(tmp_path / "sym.txt"),
+                          "-n", str(n), "-p", repr(p), "--n-planes", str(n_planes),
+                          "--z-left", repr(z_left), "--length", repr(length), "--s-z", repr(s_z),
+                          "--s-dl", repr(s_dl), "-i", "1", "-I", str(n_iter), "-o", out, *extra,
+                          str(tmp_path / "r.bin")])
+    assert rc == 0
+    naive = np.fromfile(out, np.int32).reshape(n_planes, n, n)
+    assert np.array_equal(naive, z[f"{case}_naive"])
+    img = np.fromfile(str(tmp_path / f"rho_{n_iter}.bin"), np.float32).reshape(n_planes, n, n)
+    assert rel_l2(img, z[f"{case}_rho"]) < TOL
+    assert (tmp_path / f"rho_{n_iter}.nrrd").exists() and (tmp_path / "rho.nrrd").exists()

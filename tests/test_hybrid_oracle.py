@@ -183,3 +183,33 @@ def test_hybrid_create_without_device_or_with_bad_setup(lib):
         assert lib.hybrid_ctx_create(ctypes.byref(good), 0, ctypes.byref(ctx)) == \
             _lib.STRIP_E_NODEVICE
         assert not ctx.value
+
+
+@pytest.mark.parametrize("case,kw", [("calc", {}), ("inactive", {"inactive": [3, 40]})])
+def test_cli_naive_image_matches_reference(case, kw):
+    """The drop-in CLI's naive image (Reconstruction::naive) from the kept
+    responses equals the reference's rho.bin bit for bit."""
+    from oracle import hybrid as oh
+    from stripmlem import hybrid_cli
+    z, cfg, m, resp, centers = golden_inputs()
+    n, n_planes, p, z_left = cfg[0], cfg[1], cfg[2], cfg[3]
+    res = oh.reconstruct(oracle_setup(cfg), centers, m, resp, 0, **kw)
+    img = hybrid_cli.naive_image(np.flatnonzero(res["keep"]), resp, n, n_planes, p, z_left,
+                                 centers)
+    assert np.array_equal(img, z[f"{case}_naive"])
+
+
+def test_cli_writes_reference_file_layout(tmp_path):
+    from stripmlem import hybrid_cli
+    data = np.arange(2 * 3 * 4, dtype=np.float32).reshape(4, 3, 2)
+    hybrid_cli._write_map(str(tmp_path / "rho_07"), ".bin", data, (2, 3, 4), "float")
+    assert np.array_equal(np.fromfile(tmp_path / "rho_07.bin", np.float32), data.reshape(-1))
+    hdr = open(tmp_path / "rho_07.nrrd").read()
+    assert "type: float" in hdr and "sizes: 2 3 4" in hdr and "data file: ./rho_07.bin" in hdr
+    hybrid_cli._write_map(str(tmp_path / "naive"), ".txt", data.astype(np.int32), (2, 3, 4), "int")
+    lines = open(tmp_path / "naive.txt").read().split("\n")
+    assert lines[0] == "0 1" and len([x for x in lines if x]) == 12
+    a = hybrid_cli.parse(["--system", "m", "--detector-file", "d", "-p", "0.004", "-i", "2",
+                          "-I", "5", "--inactive", "3,40", "r.bin"])
+    assert (a.blocks, a.iterations, a.responses) == (2, 5, ["r.bin"])
+    assert hybrid_cli._ints(a.inactive) == [3, 40]
