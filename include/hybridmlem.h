@@ -171,6 +171,20 @@ int hybrid_get_frames(hybrid_ctx* ctx, int32_t* lor_index, int64_t* info_begin,
 int hybrid_iterate(hybrid_ctx* ctx, int32_t n_iterations, hybrid_progress_cb progress,
                    void* user);
 
+/* One iteration split for event-sharded runs (one process per GPU, each
+ * holding a shard of the responses and the whole image): hybrid_accumulate
+ * back-projects this context's events into the accumulator (zeroed first;
+ * the caller's device buffer of n_voxels floats when hybrid_set_accumulator
+ * gave one, else the context's own), the caller sums the accumulators over
+ * the ranks (e.g. an NCCL all-reduce), and hybrid_update makes the summed
+ * accumulator the image -- the reference's sum of its per-thread images
+ * (reconstruction.h:369-376) taken across processes.  The accumulator is in
+ * the library's internal voxel order (the same on every rank); null
+ * restores the context's own. */
+int hybrid_set_accumulator(hybrid_ctx* ctx, float* device_acc);
+int hybrid_accumulate(hybrid_ctx* ctx);
+int hybrid_update(hybrid_ctx* ctx);
+
 /* The current image (n_columns * n_rows * n_planes), VoxelGrid order. */
 int hybrid_set_image(hybrid_ctx* ctx, const float* rho);
 int hybrid_get_image(hybrid_ctx* ctx, float* rho);

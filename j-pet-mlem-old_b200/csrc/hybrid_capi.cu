@@ -53,6 +53,7 @@ struct hybrid_ctx {
   float* d_acc_t = nullptr;
   float* d_tmp = nullptr;  // boundary-layout staging
   float* d_spill = nullptr;  // per-warp weight slabs of k_mlem
+  float* d_acc_user = nullptr;  // caller-owned accumulator (hybrid_set_accumulator)
   hybrid_stats stats{};
   std::string err;
 };
@@ -663,6 +664,44 @@ int hybrid_iterate(hybrid_ctx* ctx, int32_t n_iterations, hybrid_progress_cb pro
     ctx->stats.iterations++;
     if (progress) progress(ctx->stats.iterations - 1, 1, user);
   }
+  return STRIP_OK;
+}
+
+int hybrid_set_accumulator(hybrid_ctx* ctx, float* device_acc) {
+  if (!ctx) return STRIP_E_INVALID;
+  ctx->d_acc_user = device_acc;
+  return STRIP_OK;
+}
+
+int hybrid_accumulate(hybrid_ctx* ctx) {
+  if (!ctx) return STRIP_E_INVALID;
+  if (!ctx->have_sens) return fail(ctx, STRIP_E_STATE, "set the geometry and sensitivity first");
+  CK(cudaSetDevice(ctx->device));
+  float* acc = ctx->d_acc_user ? ctx->d_acc_user : ctx->d_acc_t;
+  const int blocks = ctx->sm_count * mlem_blocks_per_sm();
+  if (!ctx->d_spill) CK(cudaMalloc(&ctx->d_spill, mlem_spill_floats(blocks) * sizeof(float)));
+  CK(cudaMemsetAsync(acc, 0, ctx->n_voxels * sizeof(float), ctx->stream));
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  if (ctx->n_events > 0)
+    launch_mlem(ctx->g, geo_view(ctx), ctx->d_sens, ctx->d_frames, ctx->n_events, ctx->d_rho_t,
+                acc, ctx->d_spill, blocks, ctx->stream);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  CK(cudaEventSynchronize(ctx->ev1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  ctx->stats.last_iteration_ms = ms;
+  return STRIP_OK;
+}
+
+int hybrid_update(hybrid_ctx* ctx) {
+  if (!ctx) return STRIP_E_INVALID;
+  CK(cudaSetDevice(ctx->device));
+  const float* acc = ctx->d_acc_user ? ctx->d_acc_user : ctx->d_acc_t;
+  CK(cudaMemcpyAsync(ctx->d_rho_t, acc, ctx->n_voxels * sizeof(float), cudaMemcpyDeviceToDevice,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->stats.iterations++;
   return STRIP_OK;
 }
 

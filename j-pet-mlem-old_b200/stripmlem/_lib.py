@@ -273,6 +273,9 @@ SIGNATURES.update({
     "hybrid_get_frames": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hybrid_iterate": (ctypes.c_int, [_ctx, ctypes.c_int32, HYBRID_PROGRESS_CB, _vp]),
     "hybrid_set_image": (ctypes.c_int, [_ctx, _vp]),
+    "hybrid_set_accumulator": (ctypes.c_int, [_ctx, _vp]),
+    "hybrid_accumulate": (ctypes.c_int, [_ctx]),
+    "hybrid_update": (ctypes.c_int, [_ctx]),
     "hybrid_get_image": (ctypes.c_int, [_ctx, _vp]),
     "hybrid_get_stats": (ctypes.c_int, [_ctx, _P(HybridStats)]),
     "hybrid_generate_responses": (

@@ -73,3 +73,48 @@ class ShardedReconstruction:
 
     def close(self):
         self.rec.set_accumulator(None)
+
+
+class ShardedHybrid:
+    """The same lock-step for the 3D hybrid reconstruction: ``rec`` (a
+    stripmlem.hybrid.HybridReconstruction holding this rank's responses, or
+    an object with the same set_accumulator / accumulate / update methods and
+    n_voxels / torch_device attributes) back-projects its events into a
+    float32 accumulator, the ranks sum the accumulators, and every rank makes
+    the sum its image (the reference's sum of per-thread images,
+    src/3d/hybrid/reconstruction.h:369-376, across processes)."""
+
+    def __init__(self, rec, group=None, exchange="device"):
+        if exchange not in ("device", "host"):
+            raise ValueError("exchange must be 'device' or 'host'")
+        self.rec = rec
+        self.group = group
+        self.exchange = exchange
+        self.world = dist.get_world_size(group) if dist.is_initialized() else 1
+        self.acc = torch.zeros(rec.n_voxels, dtype=torch.float32, device=rec.torch_device)
+        rec.set_accumulator(self.acc)
+
+    def _all_reduce(self):
+        if self.world == 1:
+            return
+        if self.exchange == "device":
+            dist.all_reduce(self.acc, op=dist.ReduceOp.SUM, group=self.group)
+        else:
+            host = self.acc.cpu()
+            dist.all_reduce(host, op=dist.ReduceOp.SUM, group=self.group)
+            self.acc.copy_(host)
+        if self.acc.is_cuda:
+            torch.cuda.current_stream(self.acc.device).synchronize()
+
+    def __call__(self, n_iterations=1, progress=None):
+        for it in range(n_iterations):
+            if progress is not None:
+                progress(it, False)
+            self.rec.accumulate()
+            self._all_reduce()
+            self.rec.update()
+            if progress is not None:
+                progress(it, True)
+
+    def close(self):
+        self.rec.set_accumulator(None)

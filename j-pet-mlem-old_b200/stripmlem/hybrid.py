@@ -297,6 +297,7 @@ class HybridReconstruction:
         self.setup = _lib.HybridSetup(n_columns, n_rows, n_planes, 0, pixel_size, z_left,
                                       length, sigma_z, sigma_dl)
         self.shape = (int(n_planes), int(n_rows), int(n_columns))
+        self.device = int(device)
         ctx = ctypes.c_void_p()
         rc = self.lib.hybrid_ctx_create(ctypes.byref(self.setup), device, ctypes.byref(ctx))
         if rc != _lib.STRIP_OK:
@@ -385,6 +386,28 @@ class HybridReconstruction:
             (lambda it, fin, user: progress(it, bool(fin))) if progress else (lambda *a: None))
         self._check(self.lib.hybrid_iterate(self._ctx, n_iterations, cb, None))
         return self
+
+    # split iteration for event-sharded runs (stripmlem.distributed.ShardedHybrid)
+    @property
+    def n_voxels(self):
+        return self.shape[0] * self.shape[1] * self.shape[2]
+
+    @property
+    def torch_device(self):
+        import torch
+        return torch.device("cuda", self.device)
+
+    def set_accumulator(self, acc):
+        """acc: a CUDA float32 tensor of n_voxels on this device, or None."""
+        ptr = None if acc is None else ctypes.c_void_p(acc.data_ptr())
+        self._acc_ref = acc
+        self._check(self.lib.hybrid_set_accumulator(self._ctx, ptr))
+
+    def accumulate(self):
+        self._check(self.lib.hybrid_accumulate(self._ctx))
+
+    def update(self):
+        self._check(self.lib.hybrid_update(self._ctx))
 
     @property
     def rho(self):
