@@ -520,6 +520,11 @@ def ours(args, rank, world, local_rank):
         line["differentiable"] = diff
     if batched is not None:
         line["batched"] = batched
+    if rank == 0 and world == 1 and not args.no_hybrid:
+        # the 3D hybrid path (the next scope row, bench.py --path hybrid for the full line)
+        import bench_hybrid
+        line["hybrid"] = bench_hybrid.summary(local_rank, host_cores,
+                                              cpu_baseline=not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if shd is not None:
@@ -546,6 +551,8 @@ def main():
     ap.add_argument("--path", default="strip", choices=["strip", "hybrid"],
                     help="strip: the 2D strip MLEM headline; hybrid: the 3D hybrid MLEM")
     ap.add_argument("--hybrid-events", type=int, default=10_000_000)
+    ap.add_argument("--no-hybrid", action="store_true",
+                    help="strip path: leave out the 3D hybrid summary")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", 0))

@@ -202,3 +202,55 @@ def ours(args, rank, world, local_rank, clock_sampler, host_cores):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def summary(local_rank, host_cores, n=10_000_000, warmup=3, steps=3, e2e_iters=3,
+            cpu_baseline=True):
+    """A compact measurement of the hybrid workload for the strip bench's JSON
+    line: device-timed iterations, one end-to-end step and the reference's
+    CPU binary on a bounded sample."""
+    import ctypes
+
+    from stripmlem import _lib
+    from stripmlem import hybrid as hy
+    b, m, r = setup(n, local_rank)
+    with hy.HybridReconstruction(N_PIX, N_PIX, N_PLANES, PIXEL, Z_LEFT, LENGTH, SIGMA_Z,
+                                 SIGMA_DL, device=local_rank) as rec:
+        rec.set_geometry_from_matrix(b.centers, m)
+        rec.set_sensitivity()
+        rec.set_responses(*r)
+        st = rec.stats()
+        rec(warmup)
+        ms = []
+        for _ in range(steps):
+            rec(1)
+            ms.append(rec.stats()["last_iteration_ms"])
+        t_ms = float(sum(ms))
+        t0 = time.perf_counter()
+        rec.set_responses(*r)
+        rec(e2e_iters)
+        img = rec.rho
+        t_e2e = time.perf_counter() - t0
+        assert np.isfinite(img).all()
+    peak = ctypes.c_double()
+    if _lib.load().strip_probe_fp32_peak(local_rank, ctypes.byref(peak)) != 0:
+        peak.value = float("nan")
+    value = st["n_events"] * steps / (t_ms / 1e3) / 1e6
+    achieved = FLOPS_PER_VOXEL * st["used_voxels"] / (t_ms / steps / 1e3) / 1e12
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "steps": steps, "warmup": warmup,
+           "ms_per_step": t_ms / steps, "config": config(n, e2e_iters),
+           "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value,
+                        "unit": "TFLOP/s",
+                        "frac": achieved / peak.value if peak.value else None,
+                        "traffic": MLEM_DRAM_BYTES_PER_EVENT * st["n_events"],
+                        "model": f"{FLOPS_PER_VOXEL:.0f} flop x {st['used_voxels']} voxels"},
+           "e2e": {"value": st["n_events"] * e2e_iters / t_e2e / 1e6, "unit": UNIT,
+                   "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 4 * N_PIX * N_PIX * N_PLANES},
+           "gpu_launches": steps, "dtype": "f32", "data": "synthetic"}
+    if cpu_baseline:
+        cores = host_cores()
+        ref = run_reference(b, m, r, min(n, 2000 * cores), 2, 1, cores)
+        if ref is not None:
+            out["cpu_baseline"] = {"value": ref[0], "unit": UNIT, "cores": cores,
+                                   "kind": "reference", "sample": ref[1]}
+    return out

@@ -24,7 +24,7 @@ namespace hybridgen {
 
 constexpr int kMaxRings = 16;
 constexpr int kMaxCylinders = 32;
-constexpr uint32_t kMaxAttempts = 1u << 16;
+constexpr uint32_t kMaxAttempts = 1u << 12;  // a phantom the barrel sees fails fast
 
 struct Ring {
   int32_t first, count;  // detector index range
@@ -87,7 +87,6 @@ STRIP_HD int detect(const Setup& S, const float* poly, const float* cen, double 
 
 struct Draw {
   uint32_t v[12];
-  int used;
 };
 
 STRIP_HD void draw(uint64_t seed, int64_t i, uint32_t attempt, Draw& d) {
