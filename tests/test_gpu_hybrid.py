@@ -232,3 +232,20 @@ def test_cli_drop_in(tmp_path, case, n_iter, extra):
     img = np.fromfile(str(tmp_path / f"rho_{n_iter}.bin"), np.float32).reshape(n_planes, n, n)
     assert rel_l2(img, z[f"{case}_rho"]) < TOL
     assert (tmp_path / f"rho_{n_iter}.nrrd").exists() and (tmp_path / "rho.nrrd").exists()
+
+
+def test_twenty_iterations_against_fp64_oracle():
+    """20 iterations on the golden case stay within 1e-4 of the FP64 oracle."""
+    from oracle import hybrid as oh
+    z, cfg, m, resp, centers = golden_inputs()
+    s = oracle_setup(cfg)
+    with device_rec(cfg, centers, m) as rec:
+        rec.set_responses(*resp)
+        rec(20)
+        img = rec.rho
+        g = rec.geometry()
+        sens = rec.sensitivity
+    ora = oh.reconstruct(s, centers, m, resp, 0)
+    live = f32_live(s, ora["geo"], g["w"], sens, ora["frames"])
+    f64, _ = oh.mlem(s, ora["geo"], g["w"], sens, live, 20, f64=True)
+    assert rel_l2(img, f64) < TOL
