@@ -14,8 +14,8 @@ responses `first second z_up z_dn dl`, binary (16-byte records) or, for
 -o base.ext it writes, as the reference's CPU branch does, the naive image of
 the events' points `base.ext` (int32) and after each block
 `base_NN.ext` (binary32, or text for .txt), each with an NRRD header.
-Text responses are parsed with numpy (correctly rounded); the reference's
-fast text parser can differ from it in the last bit of a value.
+Text responses are parsed as the reference's fast text parser parses them
+(its own binary32 rounding, stripmlem.hybrid.read_responses_text).
 """
 import argparse
 import os

@@ -17,6 +17,8 @@ counts:
   calc     calculate_sensitivity, 3 iterations
   one      --sens-to-one, 2 iterations
   inactive --inactive 3,40, 2 iterations
+  text     the same responses as text in mixed number formats (text_in),
+           calculate_sensitivity, 3 iterations
 """
 import os
 import re
@@ -72,6 +74,31 @@ def main():
         out[f"{name}_naive"] = oh.ref_naive(d, s["n"], s["n_planes"])
         out[f"{name}_counts"] = counts(err)
         print(name, out[f"{name}_counts"], float(img.sum()))
+    # text responses in mixed number formats, read by the reference's fast
+    # text parser (its own binary32 rounding)
+    rng = np.random.default_rng(6)
+    fmts = ["%.9g", "%.4e", "%+.6f", "%.7g"]
+    lines = []
+    for i in range(len(r[0])):
+        f = fmts[rng.integers(0, len(fmts))]
+        lines.append(f"{int(r[0][i])} {int(r[1][i])} " +
+                     " ".join(f % float(v) for v in (r[2][i], r[3][i], r[4][i])))
+    text = "\n".join(lines) + "\n"
+    d = oh.tempdir()
+    paths = {k: os.path.join(d, f) for k, f in
+             (("m", "m.bin"), ("det", "det.txt"), ("sym", "sym.txt"), ("resp", "r.txt"))}
+    m.write(paths["m"])
+    b.write_detector_file(paths["det"])
+    hy.write_symmetry_file(paths["sym"], b.n_detectors)
+    with open(paths["resp"], "w") as f:
+        f.write(text)
+    img, err = oh.run_ref(d, paths["m"], paths["det"], paths["sym"], paths["resp"], s["n"],
+                          s["p"], s["n_planes"], s["z_left"], s["length"], s["sigma_z"],
+                          s["sigma_dl"], 3)
+    out["text_in"] = np.array(text)
+    out["text_rho"] = img
+    out["text_counts"] = counts(err)
+    print("text", out["text_counts"], float(img.sum()))
     np.savez_compressed(os.path.join(HERE, "hybrid_small.npz"), **out)
 
 

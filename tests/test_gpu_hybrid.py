@@ -249,3 +249,23 @@ def test_twenty_iterations_against_fp64_oracle():
     live = f32_live(s, ora["geo"], g["w"], sens, ora["frames"])
     f64, _ = oh.mlem(s, ora["geo"], g["w"], sens, live, 20, f64=True)
     assert rel_l2(img, f64) < TOL
+
+
+def test_cli_text_responses(tmp_path):
+    """The CLI on a text responses file (mixed number formats): within 1e-4
+    of the reference's image from the same text file."""
+    from stripmlem import hybrid as hy
+    from stripmlem import hybrid_cli
+    z, cfg, m, resp, centers = golden_inputs()
+    n, n_planes, p, z_left, length, s_z, s_dl = cfg
+    m.write(str(tmp_path / "m.bin"))
+    hy.write_detector_file(str(tmp_path / "det.txt"), z["polygons"])
+    (tmp_path / "r.txt").write_text(str(z["text_in"]))
+    out = str(tmp_path / "rho.bin")
+    assert hybrid_cli.main(["--system", str(tmp_path / "m.bin"),
+                            "--detector-file", str(tmp_path / "det.txt"), "-n", str(n),
+                            "-p", repr(p), "--n-planes", str(n_planes), "--z-left", repr(z_left),
+                            "--length", repr(length), "--s-z", repr(s_z), "--s-dl", repr(s_dl),
+                            "-i", "1", "-I", "3", "-o", out, str(tmp_path / "r.txt")]) == 0
+    img = np.fromfile(str(tmp_path / "rho_3.bin"), np.float32).reshape(n_planes, n, n)
+    assert rel_l2(img, z["text_rho"]) < TOL

@@ -213,3 +213,20 @@ def test_cli_writes_reference_file_layout(tmp_path):
                           "-I", "5", "--inactive", "3,40", "r.bin"])
     assert (a.blocks, a.iterations, a.responses) == (2, 5, ["r.bin"])
     assert hybrid_cli._ints(a.inactive) == [3, 40]
+
+
+def test_text_responses_parse_as_the_reference(tmp_path):
+    """Text responses (mixed number formats) read by stripmlem.hybrid's port
+    of the reference's fast text parser reproduce the reference's image
+    from the same file bit for bit through the oracle."""
+    from oracle import hybrid as oh
+    from stripmlem import hybrid as hy
+    z, cfg, m, resp, centers = golden_inputs()
+    path = tmp_path / "r.txt"
+    path.write_text(str(z["text_in"]))
+    parsed = hy.read_responses(str(path))
+    assert np.array_equal(parsed[0], resp[0]) and np.array_equal(parsed[1], resp[1])
+    res = oh.reconstruct(oracle_setup(cfg), centers, m, parsed, 3)
+    assert np.array_equal(res["rho"], z["text_rho"])
+    st = res["stats"]
+    assert [st["used_events"], st["used_pixels"], st["used_voxels"]] == list(z["text_counts"])
