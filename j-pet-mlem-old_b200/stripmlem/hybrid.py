@@ -646,3 +646,102 @@ def convert_tbednarski(lines, relative_time=False):
     zd = 0.5 * _C_SCINT_PS * (tdl - tdr)
     dl = 0.5 * _C_PS * ((tul + tur) - (tdl + tdr))
     return (du - 1).astype(np.int16), (dd - 1).astype(np.int16), zu, zd, dl
+
+
+# --- LOR geometry files (2d_barrel_geometry output, the --geometry input) ---------
+
+_PETg = struct.unpack("<I", b"PETg")[0]
+_PIXEL_INFO = np.dtype([("x", "<i2"), ("y", "<i2"), ("t", "<f4"), ("distance", "<f4"),
+                        ("fill", "<f4"), ("weight", "<f4")])
+
+
+def read_geometry(path):
+    """A binary32 LOR geometry file (Geometry(util::ibstream&),
+    src/2d/barrel/geometry.h: magic "PETg", n_detectors, the pixel grid,
+    then per LOR its pair, segment start / end, width and pixel infos
+    (pixel, t, distance, fill, weight)) -> dict with 'n_detectors',
+    'grid' (n_columns, n_rows, pixel_size, lower_left x, y) and 'lors'
+    {lor index: (segment (4,), width, pixel-info array)}."""
+    data = open(path, "rb").read()
+    magic, = struct.unpack_from("<I", data, 0)
+    if magic != _PETg:
+        raise ValueError("unknown binary geometry file")
+    n_det, nc, nr, p, llx, lly = struct.unpack_from("<hhhfff", data, 4)
+    off = 4 + 2 + 2 + 2 + 12
+    lors = {}
+    while off + 32 <= len(data):
+        first, second, sx, sy, ex, ey, width, n = struct.unpack_from("<hhfffffQ", data, off)
+        off += 32
+        infos = np.frombuffer(data, _PIXEL_INFO, n, off).copy()
+        off += 20 * n
+        lors[first * (first + 1) // 2 + second] = (np.array([sx, sy, ex, ey], np.float32),
+                                                   np.float32(width), infos)
+    return {"n_detectors": int(n_det), "grid": (int(nc), int(nr), float(p), float(llx),
+                                                 float(lly)), "lors": lors}
+
+
+def write_geometry(path, n_detectors, grid, lors):
+    """The inverse of read_geometry: every LOR of the table in index order
+    (empty ones included, as Geometry's operator<< writes them)."""
+    nc, nr, p, llx, lly = grid
+    n_lors = (n_detectors + 1) * n_detectors // 2
+    with open(path, "wb") as out:
+        out.write(struct.pack("<Ihhhfff", _PETg, n_detectors, nc, nr, p, llx, lly))
+        for first in range(n_detectors):
+            for second in range(first + 1):
+                li = first * (first + 1) // 2 + second
+                seg, width, infos = lors.get(li, (np.zeros(4, np.float32), 0.0,
+                                                  np.zeros(0, _PIXEL_INFO)))
+                out.write(struct.pack("<hhfffffQ", first, second, *[float(v) for v in seg],
+                                      float(width), len(infos)))
+                out.write(np.asarray(infos, _PIXEL_INFO).tobytes())
+
+
+def geometry_soa_from_file(geom, matrix=None):
+    """GeometrySOA(Geometry) (geometry_soa.h:184-205: LORs in index order,
+    pixel infos as stored, positions t, weights as stored) and, with a
+    matrix, load_weights_from_matrix_file (geometry_soa.h:207-260: weights
+    zeroed, then hits / n_emissions added to the info of each matrix element's
+    pixel in its LOR) -> dict of flat arrays for HybridReconstruction.set_geometry_soa."""
+    nd = geom["n_detectors"]
+    n_lors = (nd + 1) * nd // 2
+    seg = np.zeros((n_lors, 4), np.float32)
+    lb = np.zeros(n_lors, np.uint64)
+    le = np.zeros(n_lors, np.uint64)
+    parts = []
+    size = 0
+    for li in range(n_lors):
+        if li in geom["lors"]:
+            sg, _, infos = geom["lors"][li]
+            seg[li] = sg
+            lb[li] = size
+            parts.append(infos)
+            size += len(infos)
+            le[li] = size
+    infos = np.concatenate(parts) if parts else np.zeros(0, _PIXEL_INFO)
+    pix = np.stack([infos["x"], infos["y"]], 1).astype(np.int16)
+    pos = infos["t"].astype(np.float32)
+    w = infos["weight"].astype(np.float32).copy()
+    if matrix is not None:
+        w[:] = 0
+        f32 = np.float32
+        n_em = f32(matrix.n_emissions)
+        first = np.maximum(matrix.lor_a, matrix.lor_b).astype(np.int64)
+        second = np.minimum(matrix.lor_a, matrix.lor_b).astype(np.int64)
+        order = np.lexsort((matrix.px, matrix.py, second, first))
+        cur, idx, k, k_end = -1, None, 0, 0
+        for e in order:
+            li = int(first[e] * (first[e] + 1) // 2 + second[e])
+            if li != cur:
+                cur = li
+                b0, b1 = int(lb[li]), int(le[li])
+                idx = b0 + np.lexsort((pix[b0:b1, 0], pix[b0:b1, 1]))  # by y then x
+                k, k_end = 0, b1 - b0
+            px, py = int(matrix.px[e]), int(matrix.py[e])
+            while k < k_end and (pix[idx[k], 1], pix[idx[k], 0]) < (py, px):
+                k += 1
+            if k == k_end or (py, px) < (pix[idx[k], 1], pix[idx[k], 0]):
+                continue
+            w[idx[k]] = f32(w[idx[k]] + f32(f32(matrix.hits[e]) / n_em))
+    return {"n_detectors": nd, "segments": seg, "pixels": pix, "positions": pos, "weights": w,
+            "lor_begin": lb, "lor_end": le}

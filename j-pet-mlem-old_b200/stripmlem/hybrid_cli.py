@@ -33,11 +33,13 @@ def _ints(text):
 def parse(argv=None):
     ap = argparse.ArgumentParser(prog="3d_hybrid_reconstruction")
     ap.add_argument("--system", "-s", required=True, help="system matrix file (full form)")
-    ap.add_argument("--detector-file", required=True, help="detector description file")
+    ap.add_argument("--detector-file", default=None, help="detector description file")
+    ap.add_argument("--geometry", default=None,
+                    help="LOR geometry file (weights from --system)")
     ap.add_argument("--detector-file-sym", default=None,
                     help="detector symmetries description file (accepted, not used)")
     ap.add_argument("--n-pixels", "-n", type=int, default=None)
-    ap.add_argument("--s-pixel", "-p", type=float, required=True)
+    ap.add_argument("--s-pixel", "-p", type=float, default=None)
     ap.add_argument("--n-planes", type=int, default=None)
     ap.add_argument("--z-left", type=float, default=None)
     ap.add_argument("--length", "-l", type=float, default=2.0)
@@ -80,7 +82,19 @@ def _write_map(base, ext, data, dims, kind):
                    "ascii" if ext == ".txt" else "raw"))
 
 
-def naive_image(kept, resp, n, n_planes, p, z_left, centers):
+def lor_segments(centers):
+    """Per LOR index first * (first + 1) / 2 + second: the segment from the
+    centre of detector `second` to that of `first` (start x, y, end x, y)."""
+    c = np.asarray(centers, np.float32)
+    nd = len(c)
+    seg = np.zeros(((nd + 1) * nd // 2, 4), np.float32)
+    for a in range(nd):
+        for b in range(a + 1):
+            seg[a * (a + 1) // 2 + b] = (c[b, 0], c[b, 1], c[a, 0], c[a, 1])
+    return seg
+
+
+def naive_image(kept, resp, n, n_planes, p, z_left, segments):
     """Reconstruction::naive (reconstruction.h:394-405): the count of kept
     events per voxel of their point (the LOR's mid point + up along it, z =
     right), binary32 as the reference computes it.  kept: the kept responses'
@@ -89,7 +103,8 @@ def naive_image(kept, resp, n, n_planes, p, z_left, centers):
     idx = np.asarray(kept, np.int64)
     first, second = resp[0][idx].astype(np.int64), resp[1][idx].astype(np.int64)
     zu, zd, dl = (np.asarray(a, f32)[idx] for a in resp[2:])
-    cs, ce = centers[second].astype(f32), centers[first].astype(f32)
+    sg = np.asarray(segments, f32)[first * (first + 1) // 2 + second]
+    cs, ce = sg[:, 0:2], sg[:, 2:4]
     mid = (cs + ce) / f32(2)
     v = ce - cs
     ln = np.sqrt(v[:, 0] * v[:, 0] + v[:, 1] * v[:, 1])
@@ -113,23 +128,45 @@ def naive_image(kept, resp, n, n_planes, p, z_left, centers):
 def main(argv=None):
     a = parse(argv)
     m = hy.SystemMatrix.read(a.system)
-    n = a.n_pixels or m.n_pixels_in_row
+    inactive = _ints(a.inactive) if a.inactive else None
+    geom = None
+    if a.geometry:
+        # run_with_geometry (reconstruction_cmd.cpp:281-363): the grid from the
+        # file, the weights from the matrix
+        geom = hy.read_geometry(a.geometry)
+        nc, nr, gp, llx, lly = geom["grid"]
+        if abs(llx + gp * nc / 2) > 1e-6 * gp or abs(lly + gp * nr / 2) > 1e-6 * gp:
+            raise SystemExit("the geometry's pixel grid must be centred on the origin")
+        n = a.n_pixels or max(nc, nr)
+        if a.s_pixel is None:
+            a.s_pixel = gp
+    else:
+        if a.s_pixel is None or a.detector_file is None:
+            raise SystemExit("--s-pixel and --detector-file are required with --system")
+        n = a.n_pixels or m.n_pixels_in_row
+        nc = nr = n
     n_planes = a.n_planes if a.n_planes is not None else n
     z_left = a.z_left if a.z_left is not None else -n_planes * a.s_pixel / 2
-    polygons = hy.read_detector_file(a.detector_file)
-    if len(polygons) != m.n_detectors:
-        raise SystemExit("n_detectors mismatch")
-    centers = hy.detector_centers(polygons)
-    inactive = _ints(a.inactive) if a.inactive else None
     if a.verbose:
-        print(f"3D hybrid reconstruction w/system matrix:\n    detectors = {m.n_detectors}",
-              file=sys.stderr)
-        print(f"   pixel grid = {n} x {n} / {a.s_pixel}", file=sys.stderr)
-    rec = hy.HybridReconstruction(n, n, n_planes, a.s_pixel, z_left, a.length, a.s_z, a.s_dl,
+        print(f"3D hybrid reconstruction:\n    detectors = {m.n_detectors}", file=sys.stderr)
+        print(f"   pixel grid = {nc} x {nr} / {a.s_pixel}", file=sys.stderr)
+    rec = hy.HybridReconstruction(nc, nr, n_planes, a.s_pixel, z_left, a.length, a.s_z, a.s_dl,
                                   device=a.cuda_device)
-    rec.set_geometry_from_matrix(centers, m, inactive)
+    if geom is not None:
+        soa = hy.geometry_soa_from_file(geom, m)
+        rec.set_geometry_soa(soa["n_detectors"], soa["segments"], soa["pixels"],
+                             soa["positions"], soa["weights"], soa["lor_begin"],
+                             soa["lor_end"])
+        segments = soa["segments"]
+    else:
+        polygons = hy.read_detector_file(a.detector_file)
+        if len(polygons) != m.n_detectors:
+            raise SystemExit("n_detectors mismatch")
+        centers = hy.detector_centers(polygons)
+        rec.set_geometry_from_matrix(centers, m, inactive)
+        segments = lor_segments(centers)
     if a.sensitivity:
-        rec.set_sensitivity(_read_map(a.sensitivity, n * n))
+        rec.set_sensitivity(_read_map(a.sensitivity, nc * nr))
     elif a.sens_to_one:
         rec.set_sensitivity("one")
     else:
@@ -143,15 +180,15 @@ def main(argv=None):
         print(f"       events = {st['n_events']}", file=sys.stderr)
     start = 0
     if a.rho:
-        rec.rho = _read_map(a.rho, n * n * n_planes)
+        rec.rho = _read_map(a.rho, nc * nr * n_planes)
         base = os.path.splitext(a.rho)[0]
         digits = len(base) - len(base.rstrip("0123456789"))
         start = int(base[len(base) - digits:]) if digits else 0
     out_base, out_ext = os.path.splitext(a.output) if a.output else (None, None)
-    dims = (n, n, n_planes)
+    dims = (nc, nr, n_planes)
     if out_base:
-        _write_map(out_base, out_ext, naive_image(rec.frames()["index"], resp, n, n_planes,
-                                                  a.s_pixel, z_left, centers), dims, "int")
+        _write_map(out_base, out_ext, naive_image(rec.frames()["index"], resp, nc, n_planes,
+                                                  a.s_pixel, z_left, segments), dims, "int")
     n_total = a.blocks * a.iterations
     digits = len(str(n_total)) if n_total > 0 else 1
     for block in range(a.blocks):

@@ -96,6 +96,28 @@ def soa_from_matrix(s, centers, matrix, inactive=None):
             "lbeg": lb, "lend": le}
 
 
+def segments9(seg4):
+    """LineSegment(start, end) per LOR in binary32 (line_segment.h:18-27):
+    start, end, mid point, direction, length -- the 9-float layout."""
+    q = np.asarray(seg4, np.float32).reshape(-1, 4)
+    sx, sy, ex, ey = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    vx, vy = ex - sx, ey - sy
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ln = np.sqrt(vx * vx + vy * vy)
+        out = np.stack([sx, sy, ex, ey, (sx + ex) / np.float32(2), (sy + ey) / np.float32(2),
+                        vx / ln, vy / ln, np.sqrt(vx * vx + vy * vy)], 1)
+    return out.astype(np.float32)
+
+
+def geo_from_soa(soa):
+    """The oracle's geometry dict from flat GeometrySOA arrays."""
+    return {"seg": segments9(soa["segments"]), "pix": np.ascontiguousarray(soa["pixels"], np.int16),
+            "pos": np.ascontiguousarray(soa["positions"], np.float32),
+            "w": np.ascontiguousarray(soa["weights"], np.float32),
+            "lbeg": np.asarray(soa["lor_begin"], np.int64),
+            "lend": np.asarray(soa["lor_end"], np.int64)}
+
+
 def sensitivity(s, geo):
     sens = np.zeros((s.n_rows, s.n_columns), np.float32)
     lib().hyb_sensitivity(ctypes.byref(s), len(geo["w"]), _p(geo["pix"]), _p(geo["w"]),

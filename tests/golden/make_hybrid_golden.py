@@ -17,6 +17,9 @@ counts:
   calc     calculate_sensitivity, 3 iterations
   one      --sens-to-one, 2 iterations
   inactive --inactive 3,40, 2 iterations
+  geom     --geometry: a LOR geometry file of the same flattened geometry
+           (tests rebuild it with write_golden_geometry), weights loaded from
+           the matrix, 3 iterations
   text     the same responses as text in mixed number formats (text_in),
            calculate_sensitivity, 3 iterations
 """
@@ -41,6 +44,27 @@ CASES = {"calc": (3, ()), "one": (2, ("--sens-to-one",)), "inactive": (2, ("--in
 def counts(stderr):
     g = lambda k: int(re.search(rf"{k} count = (\d+)", stderr).group(1))  # noqa: E731
     return np.array([g("event"), g("pixel"), g("voxel")], np.int64)
+
+
+def write_golden_geometry(path, b, m):
+    """The LOR geometry file of the --geometry case: the oracle's flattened
+    geometry of the matrix (segments between detector centres, pixel infos
+    sorted by position), distance 0, fill 1, weight 0."""
+    s = SETUP
+    setup = oh.setup(s["n"], s["n"], s["n_planes"], s["p"], s["z_left"], s["length"],
+                     s["sigma_z"], s["sigma_dl"])
+    geo = oh.soa_from_matrix(setup, b.centers, m)
+    lors = {}
+    for li in range(len(geo["lbeg"])):
+        lb, le = int(geo["lbeg"][li]), int(geo["lend"][li])
+        infos = np.zeros(le - lb, hy._PIXEL_INFO)
+        infos["x"], infos["y"] = geo["pix"][lb:le, 0], geo["pix"][lb:le, 1]
+        infos["t"] = geo["pos"][lb:le]
+        infos["fill"] = 1.0
+        lors[li] = (geo["seg"][li, :4], 0.0, infos)
+    p = np.float32(s["p"])
+    ll = float(-p * np.float32(s["n"]) / np.float32(2))
+    hy.write_geometry(path, b.n_detectors, (s["n"], s["n"], s["p"], ll, ll), lors)
 
 
 def main():
@@ -74,6 +98,23 @@ def main():
         out[f"{name}_naive"] = oh.ref_naive(d, s["n"], s["n_planes"])
         out[f"{name}_counts"] = counts(err)
         print(name, out[f"{name}_counts"], float(img.sum()))
+    # the --geometry path: a LOR geometry file holding the calc case's
+    # flattened geometry (weights left 0), the weights loaded from the matrix
+    geom_path = os.path.join(oh.tempdir(), "g.bin")
+    write_golden_geometry(geom_path, b, m)
+    d = oh.tempdir()
+    paths = {k: os.path.join(d, f) for k, f in
+             (("m", "m.bin"), ("det", "det.txt"), ("sym", "sym.txt"), ("resp", "r.bin"))}
+    m.write(paths["m"])
+    b.write_detector_file(paths["det"])
+    hy.write_symmetry_file(paths["sym"], b.n_detectors)
+    hy.write_responses(paths["resp"], *r)
+    img, err = oh.run_ref(d, paths["m"], paths["det"], paths["sym"], paths["resp"], s["n"],
+                          s["p"], s["n_planes"], s["z_left"], s["length"], s["sigma_z"],
+                          s["sigma_dl"], 3, extra=("--geometry", geom_path))
+    out["geom_rho"] = img
+    out["geom_counts"] = counts(err)
+    print("geometry", out["geom_counts"], float(img.sum()))
     # text responses in mixed number formats, read by the reference's fast
     # text parser (its own binary32 rounding)
     rng = np.random.default_rng(6)

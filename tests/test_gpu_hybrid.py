@@ -8,6 +8,8 @@
 * images are within 1e-4 relative L2 of the FP64 oracle and of the
   reference's own images (tests/golden/hybrid_small.npz);
 * the device response generator equals the host generator."""
+import os
+
 import numpy as np
 import pytest
 
@@ -269,3 +271,32 @@ def test_cli_text_responses(tmp_path):
                             "-i", "1", "-I", "3", "-o", out, str(tmp_path / "r.txt")]) == 0
     img = np.fromfile(str(tmp_path / "rho_3.bin"), np.float32).reshape(n_planes, n, n)
     assert rel_l2(img, z["text_rho"]) < TOL
+
+
+def test_cli_geometry_file(tmp_path):
+    """The CLI's --geometry path (a LOR geometry file, weights from the
+    matrix): within 1e-4 of the reference's image from the same files."""
+    import sys
+    from stripmlem import hybrid as hy
+    from stripmlem import hybrid_cli
+    from conftest import ROOT
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_hybrid_golden as mk
+    z, cfg, m, resp, centers = golden_inputs()
+    n, n_planes, p, z_left, length, s_z, s_dl = cfg
+
+    class B:
+        pass
+    b = B()
+    b.centers, b.n_detectors = centers, len(centers)
+    mk.write_golden_geometry(str(tmp_path / "g.bin"), b, m)
+    m.write(str(tmp_path / "m.bin"))
+    hy.write_responses(str(tmp_path / "r.bin"), *resp)
+    out = str(tmp_path / "rho.bin")
+    assert hybrid_cli.main(["--system", str(tmp_path / "m.bin"), "--geometry",
+                            str(tmp_path / "g.bin"), "--n-planes", str(n_planes),
+                            "--z-left", repr(z_left), "--length", repr(length), "--s-z", repr(s_z),
+                            "--s-dl", repr(s_dl), "-i", "1", "-I", "3", "-o", out,
+                            str(tmp_path / "r.bin")]) == 0
+    img = np.fromfile(str(tmp_path / "rho_3.bin"), np.float32).reshape(n_planes, n, n)
+    assert rel_l2(img, z["geom_rho"]) < TOL

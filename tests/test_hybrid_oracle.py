@@ -195,7 +195,7 @@ def test_cli_naive_image_matches_reference(case, kw):
     n, n_planes, p, z_left = cfg[0], cfg[1], cfg[2], cfg[3]
     res = oh.reconstruct(oracle_setup(cfg), centers, m, resp, 0, **kw)
     img = hybrid_cli.naive_image(np.flatnonzero(res["keep"]), resp, n, n_planes, p, z_left,
-                                 centers)
+                                 hybrid_cli.lor_segments(centers))
     assert np.array_equal(img, z[f"{case}_naive"])
 
 
@@ -230,3 +230,31 @@ def test_text_responses_parse_as_the_reference(tmp_path):
     assert np.array_equal(res["rho"], z["text_rho"])
     st = res["stats"]
     assert [st["used_events"], st["used_pixels"], st["used_voxels"]] == list(z["text_counts"])
+
+
+def test_geometry_file_path_reproduces_reference(tmp_path):
+    """--geometry: a LOR geometry file read and flattened by stripmlem.hybrid
+    (GeometrySOA(Geometry) and load_weights_from_matrix_file) reproduces the
+    reference's image from the same file bit for bit through the oracle."""
+    import sys
+    from oracle import hybrid as oh
+    from stripmlem import hybrid as hy
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_hybrid_golden as mk
+    z, cfg, m, resp, centers = golden_inputs()
+
+    class B:
+        pass
+    b = B()
+    b.centers, b.n_detectors = centers, len(centers)
+    path = str(tmp_path / "g.bin")
+    mk.write_golden_geometry(path, b, m)
+    soa = hy.geometry_soa_from_file(hy.read_geometry(path), m)
+    s = oracle_setup(cfg)
+    geo = oh.geo_from_soa(soa)
+    sens = oh.sensitivity(s, geo)
+    w = oh.normalize(s, geo, sens)
+    frames, keep = oh.frame_events(s, geo, w, *resp)
+    img, st = oh.mlem(s, geo, w, sens, frames, 3)
+    assert np.array_equal(img, z["geom_rho"])
+    assert [st["used_events"], st["used_pixels"], st["used_voxels"]] == list(z["geom_counts"])
