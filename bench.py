@@ -46,8 +46,9 @@ PHANTOM = [
 ]
 SEED = 20260101
 # DRAM bytes (read + write) per event of one k_tile pass, from an ncu capture
-# of this workload's first 2e7 events (profiles/k_tile_strip_c2_2e7events.md:
-# 245.0 MB read + 6.7 MB written); the traffic grows with the event count.
+# of one launch over this workload's first 2e7 events (dram__bytes_read.sum
+# 245.0 MB + dram__bytes_write.sum 6.7 MB); the traffic grows with the event
+# count.
 TILE_DRAM_BYTES_PER_EVENT = (244.954880e6 + 6.694656e6) / 2e7
 
 
@@ -158,16 +159,17 @@ class ClockSampler:
 def run_reference_cpu(n_sample, iters, warmup, cores, events=None):
     """Times the reference 2d_strip_reconstruction (oracle/_ref, built from the
     reference sources with its default flags) on the first n_sample events of
-    the workload.  Returns (Mevent*iter/s, kind, detail)."""
+    the workload.  Returns (Mevent*iter/s, kind, detail).  Without `events`
+    the sample comes from the oracle's statement of the workload generator
+    (oracle/strip_events.c, the same events bit for bit), so this arm loads
+    nothing of the product library."""
     from oracle import oracle as orc
-    import stripmlem as sm
-    sc = scanner()
-    if events is None:
-        zu, zd, dl = sm.generate_events(sc, PHANTOM, n_sample, seed=SEED)
-    else:
-        zu, zd, dl = (a[:n_sample] for a in events)
     g = orc.geometry(GEOM["radius"], GEOM["length"], GEOM["n_y"], GEOM["n_z"],
                      GEOM["p"], GEOM["p"], GEOM["s_z"], GEOM["s_dl"])
+    if events is None:
+        zu, zd, dl = orc.generate_events(g, PHANTOM, n_sample, SEED)
+    else:
+        zu, zd, dl = (a[:n_sample] for a in events)
     if orc.ref_available(nocontract=False):
         with tempfile.TemporaryDirectory() as td:
             path = os.path.join(td, "events.bin")

@@ -36,7 +36,7 @@ SEED = 20260202
 FLOPS_PER_VOXEL = 63.0
 # DRAM bytes (read + write) per frame event of one k_mlem launch, from an ncu
 # capture of the first 1e6 responses of this workload (746.3 MB read + 1345.1
-# MB written, profiles/k_mlem_hybrid_bigbarrel_1e6responses.md): frame
+# MB written, dram__bytes_read.sum / dram__bytes_write.sum of one launch): frame
 # events, LOR pixel infos and weights, and the per-warp weight slabs' lines
 # that L2 writes back before they are read again.
 MLEM_DRAM_BYTES_PER_EVENT = (746.3424e6 + 1345.082e6) / 1e6

@@ -294,9 +294,11 @@ int strip_debug_scale_item_stats(strip_ctx* ctx, float factor);
  *
  * Scratch is a fixed file-scope device array (a binary64 accumulator and a
  * binary32 sensitivity image of STRIP_NOALLOC_MAX_PIXELS entries each, 12 MiB
- * held by every GPU that loads the library until exit).  The first call on a
- * device looks up the scratch's device address, so make that first call
- * before any stream capture.  All calls share the scratch: calls that overlap
+ * held by every GPU that loads the library until exit).  The first call in a
+ * CUDA context of a device looks up the scratch's device address and caches
+ * it with the context's unique id, so make that first call before any stream
+ * capture; a call in a new context (after cudaDeviceReset, or under another
+ * driver-API context) looks it up again.  All calls share the scratch: calls that overlap
  * on the GPU race.  Images larger than STRIP_NOALLOC_MAX_PIXELS are rejected
  * with STRIP_E_INVALID, as are invalid geometries and null pointers. */
 int strip_iterate_noalloc(const strip_geometry* geometry, const float* d_z_u,

@@ -12,13 +12,18 @@
 // kNoAllocMaxPixels entries (12 MiB in total).  Every GPU that loads this
 // library holds them until the process exits.  In host code the array names
 // are host-side stand-ins, not device addresses: the device address is taken
-// with cudaGetSymbolAddress once per device, with that device current, on the
-// first call made on that device (so the first call on a device must come
-// before any stream capture), and passed to the kernels.
+// with cudaGetSymbolAddress, with the device current, on the first call made
+// in a CUDA context (so that first call must come before any stream capture),
+// cached per device together with the context's unique id, and passed to the
+// kernels.  A call in another context of the same device -- after
+// cudaDeviceReset, or under a driver-API context other than the primary one --
+// finds the id changed and looks the address up again instead of using an
+// address of a context that may be gone.
 //
 // Every call shares the scratch and leaves the last call's contents in it;
 // each call clears the accumulator before use.  Calls that overlap on the GPU
 // (on different streams, or from different host threads) race on the scratch.
+#include <cuda.h>  // CUcontext / CUresult types only; nothing links libcuda
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -34,13 +39,51 @@ __device__ __align__(256) double g_noalloc_acc[STRIP_NOALLOC_MAX_PIXELS];
 __device__ __align__(256) float g_noalloc_sens[STRIP_NOALLOC_MAX_PIXELS];
 
 std::mutex g_setup_mutex;
-double* g_acc_ptr[kMaxDevices] = {};
-float* g_sens_ptr[kMaxDevices] = {};
 
-// Device addresses of the scratch arrays on the current device.
+struct Scratch {
+  unsigned long long ctx_id;  // unique id of the context the addresses are of
+  double* acc;
+  float* sens;
+};
+Scratch g_scratch[kMaxDevices] = {};
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Unique id of the calling thread's current context (0: none, or a driver
+// without cuCtxGetId).  The driver functions come through the runtime's entry
+// point table, so the library does not link libcuda.
+unsigned long long current_ctx_id() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    looked_up = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+    cudaGetLastError();
+  }
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device addresses of the scratch arrays in the current context of `device`.
 int noalloc_scratch(int device, double** acc, float** sens) {
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_acc_ptr[device]) {
+  Scratch& c = g_scratch[device];
+  const unsigned long long id = current_ctx_id();
+  if (id == 0 || id != c.ctx_id) {
     double* a = nullptr;
     float* s = nullptr;
     if (cudaGetSymbolAddress(reinterpret_cast<void**>(&a), g_noalloc_acc) !=
@@ -48,13 +91,15 @@ int noalloc_scratch(int device, double** acc, float** sens) {
         cudaGetSymbolAddress(reinterpret_cast<void**>(&s), g_noalloc_sens) !=
             cudaSuccess) {
       cudaGetLastError();
+      c = Scratch{};
       return STRIP_E_CUDA;
     }
-    g_acc_ptr[device] = a;
-    g_sens_ptr[device] = s;
+    // the lookup makes the runtime's context current if none was; without an
+    // id (no driver support) nothing is cached and every call looks up again
+    c = Scratch{current_ctx_id(), a, s};
   }
-  *acc = g_acc_ptr[device];
-  *sens = g_sens_ptr[device];
+  *acc = c.acc;
+  *sens = c.sens;
   return STRIP_OK;
 }
 

@@ -80,6 +80,7 @@ def lib():
             "orc_pixel_center_f64": (None, [g, ctypes.c_int32, ctypes.c_int32, d]),
             "orc_to_projection_tan_f64": (None, [c_d, c_d, c_d, c_d, d]),
             "orc_from_projection_tan_f64": (None, [c_d, c_d, c_d, c_d, d]),
+            "orc_generate_events": (c_i, [g, d, c_i, ctypes.c_uint64, c_l, f, f, f]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -108,6 +109,20 @@ def _ip(a):
 def _soa(z_u, z_d, dl):
     return (np.ascontiguousarray(z_u, np.float32), np.ascontiguousarray(z_d, np.float32),
             np.ascontiguousarray(dl, np.float32))
+
+
+def generate_events(g, ellipses, n, seed):
+    """n seeded events (z_u, z_d, dl binary32 arrays) of the benchmark's
+    counter-based generator; ellipses = rows (z, y, a, b, angle_deg,
+    activity).  The same events as the product library's generator, computed
+    without it (strip_events.c)."""
+    el = np.ascontiguousarray(np.asarray(ellipses, np.float64).reshape(-1, 6))
+    out = [np.empty(n, np.float32) for _ in range(3)]
+    rc = lib().orc_generate_events(ctypes.byref(g), _dp(el), el.shape[0], int(seed), n,
+                                   *(_fp(a) for a in out))
+    if rc != 0:
+        raise ValueError("orc_generate_events failed")
+    return tuple(out)
 
 
 def event_box(g, z_u, z_d, dl, f64=False):

@@ -129,6 +129,15 @@ void orc_to_projection_tan_f64(double R, double y, double z, double tan,
 void orc_from_projection_tan_f64(double R, double z_u, double z_d, double dl,
                                  double out[3]);
 
+/* --- synthetic events (strip_events.c) ----------------------------------- */
+
+/* n seeded events of the benchmark's generator from ellipses given as
+ * n_ellipses rows of (z, y, a, b, angle in degrees, activity); returns 0, or
+ * -1 on bad arguments or an event no attempt could detect. */
+int orc_generate_events(const orc_geometry* g, const double* ellipses,
+                        int n_ellipses, uint64_t seed, int64_t n, float* z_u,
+                        float* z_d, float* dl);
+
 #ifdef __cplusplus
 }
 #endif
