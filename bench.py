@@ -257,6 +257,56 @@ def differentiable_throughput(rec, n, reps=2):
     return tf / reps, ta / reps
 
 
+def accuracy_vs_fp64(events, n_sample, iters, local_rank, n_subsets=1):
+    """Error of the benchmark's kernel configuration against the FP64 oracle
+    (the checker): the first n_sample events of the workload reconstructed on
+    the GPU -- MLEM with 8000-event work items, the full run's item size, or
+    n_subsets-subset OSEM -- for `iters` iterations, and the same in binary64
+    on the host (oracle/strip_oracle.c, all host threads)."""
+    import stripmlem as sm
+    from oracle import oracle as orc
+    zu, zd, dl = (a[:n_sample] for a in events)
+    g = orc.geometry(GEOM["radius"], GEOM["length"], GEOM["n_y"], GEOM["n_z"],
+                     GEOM["p"], GEOM["p"], GEOM["s_z"], GEOM["s_dl"])
+    with sm.Reconstruction(scanner(), device=local_rank, mode=sm.MODE_CPU,
+                           accumulation=sm.ACCUM_KAHAN) as r:
+        if n_subsets == 1:
+            r.set_item_events(8000)
+        r.set_events(zu, zd, dl, n_subsets=n_subsets)
+        max_item = r.stats()["max_item_events"]
+        r(None, iters, n_subsets=n_subsets)
+        img = r.rho.astype(np.float64)
+    ref = orc.mlem_f64(g, zu, zd, dl, iters, n_subsets=n_subsets, sets_f32=True)
+
+    def rel(b):
+        return float(np.linalg.norm(img - b) / np.linalg.norm(b))
+
+    out = {"rel_l2_vs_fp64": rel(ref),
+           "max_pixel_err_rel_peak": float(np.abs(img - ref).max() / np.abs(ref).max()),
+           "sample": f"first {n_sample} events of the workload, {iters} "
+                     + ("MLEM iterations, 8000-event work items (largest item "
+                        f"{max_item}), the benchmark's kernel configuration"
+                        if n_subsets == 1 else f"{n_subsets}-subset OSEM iterations")
+                     + "; FP64 oracle with the reference's binary32 pixel sets"}
+    if n_subsets == 1:
+        out["rel_l2_vs_full_fp64"] = rel(orc.mlem_f64(g, zu, zd, dl, iters, sets_f32=False))
+    return out
+
+
+def osem_throughput(rec, n, n_subsets, warmup, steps):
+    """Device time of `steps` OSEM iterations (each a sweep over all events
+    in n_subsets subset updates) on the resident events; Mevent*iter/s."""
+    rec(None, warmup, n_subsets=n_subsets)  # the first call re-bins
+    rec(None, steps, n_subsets=n_subsets)
+    st = rec.stats()
+    ms = st["last_iterate_ms"]
+    return {"subsets": n_subsets, "steps": steps, "ms_per_iteration": ms / steps,
+            "Mevent_iter_per_s": n * steps / (ms / 1e3) / 1e6,
+            "launches_per_iteration": st["kernel_launches"] / steps,
+            "what": f"{n_subsets}-subset OSEM (subset = event index mod {n_subsets}); "
+                    "an iteration visits every subset once"}
+
+
 def batch_instances(n_inst=64):
     """The batched workload: n_inst reconstructions, instance i seeded by i --
     image n_y x n_z with n in [100, 800], pixel p in {1, 2, 3, 4} mm, strips
@@ -469,6 +519,17 @@ def ours(args, rank, world, local_rank):
                 "what": "strip_forward_device then strip_adjoint_device over the same "
                         "events (y_e = sum_j K_ej rho_j, g_j = sum_e K_ej / y_e)"}
 
+    error = None
+    osem = None
+    if rank == 0 and world == 1 and args.error_events > 0:
+        error = accuracy_vs_fp64((zu, zd, dl), min(n, args.error_events), args.e2e_iters,
+                                 local_rank)
+    if world == 1 and not args.no_osem:
+        osem = osem_throughput(rec, n, 8, 1, 2)
+        if rank == 0 and args.error_events > 0:
+            osem["error"] = accuracy_vs_fp64((zu, zd, dl), min(n, args.error_events // 2), 2,
+                                             local_rank, n_subsets=8)
+
     batched = None
     achieved_plain = flops_per_iter / (tile_ms / args.steps / 1e3) / 1e12
     if world == 1 and not args.no_batched:
@@ -514,12 +575,16 @@ def ours(args, rank, world, local_rank):
                                        "halo_z", "halo_y", "n_work_items", "n_overflow",
                                        "n_empty", "smem_bytes", "last_setup_ms")},
     }
+    if error is not None:
+        line["error"] = error
     if e2e is not None:
         line["e2e"] = e2e
     if cpu is not None:
         line["cpu_baseline"] = cpu
     if diff is not None:
         line["differentiable"] = diff
+    if osem is not None:
+        line["osem8"] = osem
     if batched is not None:
         line["batched"] = batched
     if rank == 0 and world == 1 and not args.no_hybrid:
@@ -550,6 +615,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-differentiable", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-osem", action="store_true")
+    ap.add_argument("--error-events", type=int, default=1_000_000,
+                    help="events of the prefix whose 20-iteration image is checked "
+                         "against the FP64 oracle (0: no check)")
     ap.add_argument("--path", default="strip", choices=["strip", "hybrid"],
                     help="strip: the 2D strip MLEM headline; hybrid: the 3D hybrid MLEM")
     ap.add_argument("--hybrid-events", type=int, default=10_000_000)

@@ -103,6 +103,8 @@ typedef struct strip_stats {
   int64_t n_fallback;        /* events of the last strip_iterate / accumulate
                                 that a tile's unweighted fixed-point window had
                                 no room for (rerun in a weighted window)       */
+  int32_t max_item_events;   /* events of the largest tile work item           */
+  int32_t reserved;
 } strip_stats;
 
 /* ---- context ------------------------------------------------------------ */
@@ -253,6 +255,13 @@ int strip_autotune(strip_ctx* ctx, int mode, strip_tuning* best);
 /* Sets the schedule by hand (tile edge 8..128, grab 1..32); re-bins the
  * events when the context has some.  Defaults: tile 32, grab 32. */
 int strip_set_schedule(strip_ctx* ctx, int tile, int grab);
+/* Largest tile work item, in events (1..8000); 0 (the default) picks it per
+ * binning: enough items for about eight waves of the device, at least 2048
+ * and at most 8000 events.  Re-bins the events when the context has some.
+ * The item size changes the work decomposition and the fixed-point scale of
+ * each item's window, not the result beyond rounding; a small event set
+ * binned with 8000-event items runs the arithmetic of a large one. */
+int strip_set_item_events(strip_ctx* ctx, int max_events);
 
 /* ---- parity ----------------------------------------------------------- */
 

@@ -328,4 +328,13 @@ int strip_set_schedule(strip_ctx* ctx, int tile, int grab) {
   return ctx_rebin(ctx, tile);
 }
 
+int strip_set_item_events(strip_ctx* ctx, int max_events) {
+  if (!ctx) return STRIP_E_INVALID;
+  if (max_events < 0 || max_events > kMaxItemEvents)
+    return ctx_fail(ctx, STRIP_E_INVALID, "strip_set_item_events: 0 or 1..8000 events");
+  ctx->item_events = max_events;
+  if (ctx->n_subsets <= 0) return STRIP_OK;  // used by the next binning
+  return ctx_rebin(ctx, ctx->tile_pref);
+}
+
 }  // extern "C"

@@ -259,8 +259,11 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
   std::vector<int64_t> gb(n_subsets), gc(n_subsets);
   const int64_t per_sub = (int64_t)(total / (unsigned long long)n_subsets) + 1;
   const int64_t target = (int64_t)ctx->sm_count * 2 * 8;
-  const int64_t chunk = std::min<int64_t>(
-      kMaxItemEvents, std::max<int64_t>(2048, per_sub / target + 1));
+  const int64_t chunk =
+      ctx->item_events > 0
+          ? std::min<int64_t>(kMaxItemEvents, ctx->item_events)
+          : std::min<int64_t>(kMaxItemEvents,
+                              std::max<int64_t>(2048, per_sub / target + 1));
   for (int sb = 0; sb < n_subsets; ++sb) {
     ib[sb] = (int)items.size();
     for (int64_t round = 0;; ++round) {
@@ -354,6 +357,9 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
   S.halo_z = t.HX;
   S.halo_y = t.HY;
   S.n_work_items = (int32_t)ctx->items.size();
+  S.max_item_events = 0;
+  for (const WorkItem& w : ctx->items)
+    S.max_item_events = std::max(S.max_item_events, w.count);
   S.n_subsets = n_subsets;
   S.max_box_w = wh[0];
   S.max_box_h = wh[1];

@@ -243,6 +243,11 @@ class Reconstruction:
     def set_schedule(self, tile=32, grab=32):
         self._check(self.lib.strip_set_schedule(self._ctx, int(tile), int(grab)))
 
+    def set_item_events(self, max_events=0):
+        """Largest tile work item in events (1..8000), or 0 to let each
+        binning choose (strip_set_item_events)."""
+        self._check(self.lib.strip_set_item_events(self._ctx, int(max_events)))
+
     # -- split iteration (events sharded over processes) -------------------
     def set_accumulator(self, acc):
         """Makes ``acc`` (a float64 CUDA tensor of n_y * n_z values on this

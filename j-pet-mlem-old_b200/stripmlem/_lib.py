@@ -91,6 +91,8 @@ class Stats(ctypes.Structure):
         ("last_setup_ms", ctypes.c_double),
         ("last_tile_ms", ctypes.c_double),
         ("n_fallback", ctypes.c_int64),
+        ("max_item_events", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 
@@ -165,6 +167,7 @@ SIGNATURES = {
     "strip_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "strip_autotune": (ctypes.c_int, [_ctx, ctypes.c_int, _P(Tuning)]),
     "strip_set_schedule": (ctypes.c_int, [_ctx, ctypes.c_int, ctypes.c_int]),
+    "strip_set_item_events": (ctypes.c_int, [_ctx, ctypes.c_int]),
     "strip_debug_pixel_sets": (
         ctypes.c_int,
         [_ctx, _f, _f, _f, ctypes.c_int64, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_uint64)],

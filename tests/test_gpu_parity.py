@@ -125,18 +125,19 @@ def test_mlem_gpu_mode_vs_fp64(c1):
     assert rel_l2(img, ref) < REL_L2_TOL
 
 
-def test_osem_subsets_vs_fp64(c1):
+@pytest.mark.parametrize("n_subsets", [4, 8])
+def test_osem_subsets_vs_fp64(c1, n_subsets):
     import stripmlem as sm
     sc, g, (zu, zd, dl) = c1
     n = 40_000
     with sm.Reconstruction(sc) as rec:
-        rec.set_events(zu[:n], zd[:n], dl[:n], n_subsets=4)
-        rec(None, 3)
+        rec.set_events(zu[:n], zd[:n], dl[:n], n_subsets=n_subsets)
+        rec(None, 3, n_subsets=n_subsets)
         img = rec.rho
         # back to full-set MLEM on the same context: re-binning path
         rec(None, 1, n_subsets=1)
         img2 = rec.rho
-    ref = orc.mlem_f64(g, zu[:n], zd[:n], dl[:n], 3, n_subsets=4, sets_f32=True)
+    ref = orc.mlem_f64(g, zu[:n], zd[:n], dl[:n], 3, n_subsets=n_subsets, sets_f32=True)
     assert rel_l2(img, ref) < REL_L2_TOL
     ref2 = orc.mlem_f64(g, zu[:n], zd[:n], dl[:n], 1, rho=ref, sets_f32=True)
     assert rel_l2(img2, ref2) < REL_L2_TOL
