@@ -331,13 +331,17 @@ def batch_instances(n_inst=64):
     return out
 
 
-def batched_throughput(local_rank, n_inst, warmup, steps):
+def batched_throughput(local_rank, n_inst, warmup, steps, autotune=True):
     """The same instances advanced one context at a time (strip_iterate) and
-    as one batch (strip_batch_*): Mevent*iter/s of each over all events."""
+    as one batch (strip_batch_*): Mevent*iter/s of each over all events.
+    With autotune, every instance first gets its own tile / grab schedule
+    from strip_autotune (timed on its own events); both legs use it."""
     import torch
     import stripmlem as sm
     recs = []
     total = 0
+    schedules = {}
+    tune_s = 0.0
     try:
         for inst in batch_instances(n_inst):
             sc = sm.Scanner(inst["R"], inst["L"], inst["n_y"], inst["n_z"], inst["p"],
@@ -347,6 +351,12 @@ def batched_throughput(local_rank, n_inst, warmup, steps):
             rec = sm.Reconstruction(sc, device=local_rank, mode=sm.MODE_CPU)
             rec.set_events_device(*ev)
             del ev
+            if autotune:
+                t0 = time.perf_counter()
+                best = rec.autotune()
+                tune_s += time.perf_counter() - t0
+                key = f"tile{best['tile']}_grab{best['grab']}"
+                schedules[key] = schedules.get(key, 0) + 1
             recs.append(rec)
             total += inst["events"]
         torch.cuda.empty_cache()
@@ -379,6 +389,9 @@ def batched_throughput(local_rank, n_inst, warmup, steps):
                 "events_on_global_path": overflow,
                 "tile_work_items": st["n_work_items"],
                 "launches_per_step": st["launches_per_iteration"],
+                "autotuned": autotune,
+                "schedules": schedules,
+                "autotune_s": tune_s,
                 "what": "64 seeded instances (image 100-800 px per side, 1-4 mm pixels, "
                         "1e5-2e7 events each): one MLEM step of every instance as one "
                         "persistent tile launch + one update launch replayed from a CUDA "
@@ -619,8 +632,10 @@ def main():
     ap.add_argument("--error-events", type=int, default=1_000_000,
                     help="events of the prefix whose 20-iteration image is checked "
                          "against the FP64 oracle (0: no check)")
-    ap.add_argument("--path", default="strip", choices=["strip", "hybrid"],
-                    help="strip: the 2D strip MLEM headline; hybrid: the 3D hybrid MLEM")
+    ap.add_argument("--path", default="strip", choices=["strip", "hybrid", "precision"],
+                    help="strip: the 2D strip MLEM headline; hybrid: the 3D hybrid MLEM; "
+                         "precision: the accumulation-mode error study")
+    ap.add_argument("--precision-events", type=int, default=1_000_000)
     ap.add_argument("--hybrid-events", type=int, default=10_000_000)
     ap.add_argument("--no-hybrid", action="store_true",
                     help="strip path: leave out the 3D hybrid summary")
@@ -631,6 +646,11 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if world > 1 and "RANK" not in os.environ:
         sys.exit("for --gpus N > 1 launch under torchrun (one rank per GPU)")
+    if args.path == "precision":
+        import bench_precision
+        if rank != 0:
+            return 0
+        return bench_precision.run(args, local_rank, host_cores)
     if args.path == "hybrid":
         import bench_hybrid
         if args.e2e_iters == 20:

@@ -191,6 +191,14 @@ int hybrid_get_image(hybrid_ctx* ctx, float* rho);
 
 int hybrid_get_stats(hybrid_ctx* ctx, hybrid_stats* out);
 
+/* Test hook: evaluates, on CUDA device `device`, the arctangent the MLEM
+ * kernel uses for the strip frame's angular sensitivity (which = 0: atan2(a, b)
+ * for a > 0 by an odd degree-15 polynomial) or CUDA's atan2f (which = 1) on
+ * n host argument pairs; out receives n values.  The reference calls
+ * std::atan (gaussian_kernel.h:139-148); this bounds the replacement. */
+int hybrid_debug_atan2(int32_t device, const float* a, const float* b, int64_t n,
+                       int32_t which, float* out);
+
 /* A z-cylinder of a synthetic phantom: centre, radius, half length along z,
  * activity. */
 typedef struct hybrid_cylinder {

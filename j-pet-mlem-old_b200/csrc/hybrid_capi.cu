@@ -733,4 +733,33 @@ int hybrid_get_stats(hybrid_ctx* ctx, hybrid_stats* out) {
   return STRIP_OK;
 }
 
+int hybrid_debug_atan2(int32_t device, const float* a, const float* b, int64_t n,
+                       int32_t which, float* out) {
+  if (n < 0 || (n > 0 && (!a || !b || !out)) || (which != 0 && which != 1))
+    return STRIP_E_INVALID;
+  if (n == 0) return STRIP_OK;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+    cudaGetLastError();
+    return STRIP_E_NODEVICE;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) return STRIP_E_CUDA;
+  float* d = nullptr;
+  const size_t bytes = (size_t)n * sizeof(float);
+  if (cudaMalloc(&d, 3 * bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return STRIP_E_NOMEM;
+  }
+  cudaError_t e = cudaMemcpy(d, a, bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + n, b, bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = launch_atan2_probe(d, d + n, n, which, d + 2 * n, nullptr);
+  if (e == cudaSuccess) e = cudaMemcpy(out, d + 2 * n, bytes, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return STRIP_E_CUDA;
+  }
+  return STRIP_OK;
+}
+
 }  // extern "C"

@@ -78,5 +78,7 @@ size_t mlem_spill_floats(int n_blocks);
 int mlem_blocks_per_sm();
 void launch_event_counts(const Frame* frames, int64_t n, unsigned long long* out2,
                          cudaStream_t st);
+cudaError_t launch_atan2_probe(const float* a, const float* b, int64_t n, int which,
+                               float* out, cudaStream_t st);
 
 }  // namespace hybridmlem

@@ -62,23 +62,24 @@ constexpr int kUnroll2 = HYBRID_UNROLL2;         // pass-2 voxel-loop unroll
 
 // atan2(a, b) for a > 0, in (0, pi): the quotient of the smaller by the
 // larger of a and |b| (fast division) folded into [0, 1], an odd polynomial
-// t P(t^2) of degree 15 for atan on [0, 1] (coefficients fitted for this
-// kernel by iteratively reweighted least squares toward the minimax absolute
-// error: 3.8e-8 in exact arithmetic, 1.1e-7 evaluated in binary32), then the
-// quadrant.  The reference's atanf(u) - atanf(v) carries about the same
-// binary32 rounding.
+// t P(t^2) of degree 15 for atan on [0, 1], then the quadrant.  The
+// coefficients come from tests/golden/fit_atan.py: Lawson's iteratively
+// reweighted least squares toward the minimax absolute error (3.75e-8 in
+// exact arithmetic, 1.2e-7 evaluated in binary32), rounded to binary32.
+// The reference's atanf(u) - atanf(v) carries about the same binary32
+// rounding.
 __device__ __forceinline__ float atan2_pos(float a, float b) {
   const float ab = fabsf(b);
   const float mx = fmaxf(a, ab), mn = fminf(a, ab);
   const float t = __fdividef(mn, mx);
   const float s = t * t;
-  float p = -0.004054941702634096f;
-  p = fmaf(p, s, 0.021864276379346848f);
-  p = fmaf(p, s, -0.055914171040058136f);
-  p = fmaf(p, s, 0.09642327576875687f);
-  p = fmaf(p, s, -0.1390867829322815f);
-  p = fmaf(p, s, 0.19946575164794922f);
-  p = fmaf(p, s, -0.33329862356185913f);
+  float p = -0.0040545654483139515f;
+  p = fmaf(p, s, 0.021862952038645744f);
+  p = fmaf(p, s, -0.0559123195707798f);
+  p = fmaf(p, s, 0.0964219719171524f);
+  p = fmaf(p, s, -0.1390862911939621f);
+  p = fmaf(p, s, 0.19946566224098206f);
+  p = fmaf(p, s, -0.33329859375953674f);
   p = fmaf(p, s, 0.9999993443489075f);
   float r = t * p;
   if (a > ab) r = 1.5707963267948966f - r;
@@ -331,6 +332,24 @@ void launch_event_counts(const Frame* frames, int64_t n, unsigned long long* out
                          cudaStream_t st) {
   cudaMemsetAsync(out2, 0, 2 * sizeof(unsigned long long), st);
   k_event_counts<<<grid_for(n), 256, 0, st>>>(frames, n, out2);
+}
+
+namespace {
+// The kernel's arctangent (which = 0) or CUDA's atan2f (which = 1) on n
+// argument pairs: the test hook that bounds atan2_pos's error.
+__global__ void k_atan2_probe(const float* a, const float* b, int64_t n, int which,
+                              float* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = which == 0 ? atan2_pos(a[i], b[i]) : atan2f(a[i], b[i]);
+}
+}  // namespace
+
+cudaError_t launch_atan2_probe(const float* a, const float* b, int64_t n, int which,
+                               float* out, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  k_atan2_probe<<<grid_for(n), 256, 0, st>>>(a, b, n, which, out);
+  return cudaGetLastError();
 }
 
 }  // namespace hybridmlem

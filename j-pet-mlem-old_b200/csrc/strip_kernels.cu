@@ -624,7 +624,10 @@ __device__ __forceinline__ float process_event(const LaunchArgs& a,
   float scale;
   if (OP == OP_MLEM || OP == OP_FORWARD) {
     RowSum<ACC> acc;
-    for (int r0 = 0; r0 < H; r0 += kSuper) {
+    // super-blocks of rows last to first, so that the registers end holding
+    // the first (the middle rows, the longest runs): pass 2 rebuilds only
+    // the others
+    for (int r0 = ((H - 1) / kSuper) * kSuper; r0 >= 0; r0 -= kSuper) {
       build_lane_rows<MODE>(a.s, a.k, e, er, ge, H, r0, lane, win, L);
       pass1_rows<MODE, ACC>(a.s, a.k, e, H, r0, lane, L,
                             min(kRowBlocks, (H - r0 + 31) >> 5), win, acc);
@@ -655,12 +658,12 @@ __device__ __forceinline__ float process_event(const LaunchArgs& a,
     if (!__shfl_sync(kFull, ok, 0)) return -scale;
   }
   constexpr bool kWeighted = OP == OP_MLEM && MODE == STRIP_MODE_CPU;
-  if ((OP == OP_MLEM) && H <= kSuper) {
-    pass2_rows<MODE, kWeighted>(a.s, a.k, e, H, 0, lane, L, (H + 31) >> 5, win,
-                                scale);
-    return scale;
+  if (OP == OP_MLEM) {  // the registers hold the first super-block
+    pass2_rows<MODE, kWeighted>(a.s, a.k, e, H, 0, lane, L,
+                                min(kRowBlocks, (H + 31) >> 5), win, scale);
+    if (H <= kSuper) return scale;
   }
-  for (int r0 = 0; r0 < H; r0 += kSuper) {
+  for (int r0 = OP == OP_MLEM ? kSuper : 0; r0 < H; r0 += kSuper) {
     build_lane_rows<MODE>(a.s, a.k, e, er, ge, H, r0, lane, win, L);
     pass2_rows<MODE, kWeighted>(a.s, a.k, e, H, r0, lane, L,
                                 min(kRowBlocks, (H - r0 + 31) >> 5), win, scale);

@@ -281,6 +281,8 @@ SIGNATURES.update({
     "hybrid_update": (ctypes.c_int, [_ctx]),
     "hybrid_get_image": (ctypes.c_int, [_ctx, _vp]),
     "hybrid_get_stats": (ctypes.c_int, [_ctx, _P(HybridStats)]),
+    "hybrid_debug_atan2": (ctypes.c_int, [ctypes.c_int32, _vp, _vp, ctypes.c_int64,
+                                          ctypes.c_int32, _vp]),
     "hybrid_generate_responses": (
         ctypes.c_int,
         [ctypes.c_int32, _vp, _P(HybridCylinder), ctypes.c_int32, ctypes.c_double,

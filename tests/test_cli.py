@@ -206,3 +206,61 @@ def test_phantom_cli_emissions_and_shapes(tmp_path):
     z, y = 10.0, 20.0
     col, row = int(np.floor((z + 250) / 2)), int(np.floor((y + 200) / 2))
     assert emi[row, col] > 0.8 * 30000 * 5000 / total_w
+
+
+REF_PHANTOM = os.path.join(ROOT, "oracle", "_ref", "2d_strip_phantom")
+
+
+def _two_sample_chi2(a, b, min_count=20):
+    """Chi-squared two-sample test of two histograms with the same bins
+    (bins holding fewer than min_count events together are pooled)."""
+    from scipy import stats
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    keep = (a + b) >= min_count
+    a = np.append(a[keep], a[~keep].sum())
+    b = np.append(b[keep], b[~keep].sum())
+    if a[-1] + b[-1] == 0:
+        a, b = a[:-1], b[:-1]
+    ka, kb = np.sqrt(b.sum() / a.sum()), np.sqrt(a.sum() / b.sum())
+    chi2 = float(np.sum((ka * a - kb * b) ** 2 / (a + b)))
+    return chi2, float(stats.chi2.sf(chi2, len(a) - 1))
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.access(REF_PHANTOM, os.X_OK),
+                    reason="the reference's 2d_strip_phantom was not built")
+def test_phantom_cli_matches_reference_generator_in_distribution(tmp_path):
+    """The drop-in 2d_strip_phantom (Philox streams, on the GPU) against the
+    reference's own (tausworthe, src/2d/strip/phantom_cmd.cpp; the Monte
+    Carlo of src/common/phantom_monte_carlo.h:29-109 and
+    src/2d/geometry/phantom.h:183-215, uniform emission angle) on the same
+    phantom and options: 1e6 detected events each, two-sample
+    Kolmogorov-Smirnov tests on z_u, z_d and dl and chi-squared tests on the
+    detected- and emitted-point images.  Both runs are seeded (the
+    reference's generators are default-seeded with one thread), so the test
+    is deterministic; the bar is p > 1e-3."""
+    from scipy import stats
+    ph = tmp_path / "phantom"
+    ph.write_text("".join(f"ellipse {z} {y} {a} {b} {ang} {act}\n"
+                          for z, y, a, b, ang, act in C1_PHANTOM_T)
+                  + "rectangle -120 -60 20 15 0.5\n")
+    n = 1_000_000
+    ref = subprocess.run([REF_PHANTOM, str(ph), *C1_ARGS, "-e", str(n), "--detected",
+                          "-T", "1", "-o", str(tmp_path / "ref.bin")],
+                         capture_output=True, text=True, timeout=600, cwd=tmp_path)
+    assert ref.returncode == 0, ref.stderr[-500:]
+    run_phantom(ph, *C1_ARGS, "-e", n, "--detected", "--seed", "3",
+                "-o", tmp_path / "ours.bin")
+    a = np.fromfile(tmp_path / "ref.bin", dtype="<f4").reshape(-1, 3)
+    b = np.fromfile(tmp_path / "ours.bin", dtype="<f4").reshape(-1, 3)
+    assert abs(a.shape[0] - n) <= 64 and b.shape[0] == n
+    for k, name in enumerate(("z_u", "z_d", "dl")):
+        p = stats.ks_2samp(a[:, k], b[:, k]).pvalue
+        assert p > 1e-3, (name, p)
+    for img in ("detected", "emitted"):
+        ia = np.fromfile(tmp_path / f"ref_{img}", dtype="<i4")
+        ib = np.fromfile(tmp_path / f"ours_{img}", dtype="<i4")
+        assert ia.shape == ib.shape
+        _, p = _two_sample_chi2(ia, ib)
+        assert p > 1e-3, (img, p)

@@ -63,8 +63,9 @@ def test_c2_mlem_20_iterations_vs_fp64(c2):
     assert rel_l2(img, ref) < REL_L2_TOL
     ref64 = orc.mlem_f64(g, zu, zd, dl, 20, sets_f32=False)
     assert rel_l2(img, ref64) < 2 * REL_L2_TOL
-    # the unweighted windows were used: no event needed the weighted rerun
-    assert fallbacks == 0
+    # the unweighted windows carried the passes: the weighted rerun of events
+    # they had no room for stays rare
+    assert fallbacks < 1e-5 * N_EVENTS * 20
 
 
 def test_c2_osem_8_subsets_vs_fp64(c2):
