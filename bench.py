@@ -307,6 +307,72 @@ def osem_throughput(rec, n, n_subsets, warmup, steps):
                     "an iteration visits every subset once"}
 
 
+def write_event_file(path, zu, zd, dl, chunk=10_000_000):
+    """The events as the reference's binary event file (raw f32 triples)."""
+    with open(path, "wb") as f:
+        for a in range(0, zu.shape[0], chunk):
+            b = min(zu.shape[0], a + chunk)
+            np.stack([zu[a:b], zd[a:b], dl[a:b]], axis=1).astype("<f4").tofile(f)
+
+
+def io_throughput(zu, zd, dl, local_rank, iters):
+    """Event input from a file (page cache warm, the file just written):
+    strip_load_responses_file (file -> pinned staging -> HBM -> binning),
+    the pageable path (np.fromfile, then the AoS setter), and the drop-in CLI
+    end to end (process start, file -> HBM, `iters` iterations, image file)
+    timed by the wall clock."""
+    import stripmlem as sm
+    n = zu.shape[0]
+    d = tempfile.mkdtemp(prefix="strip_io_")
+    path = os.path.join(d, "events.bin")
+    out = {"events": n, "file_bytes": 12 * n, "page_cache": "warm (file just written)"}
+    try:
+        write_event_file(path, zu, zd, dl)
+        with sm.Reconstruction(scanner(), device=local_rank) as rec:
+            times = []
+            for _ in range(2):
+                t0 = time.perf_counter()
+                rec.load_responses_file(path)
+                times.append(time.perf_counter() - t0)
+            out["file_to_hbm_binned_s"] = min(times)
+            out["file_to_hbm_binned_GBps"] = 12 * n / min(times) / 1e9
+            out["binning_ms"] = rec.stats()["last_setup_ms"]
+            t0 = time.perf_counter()
+            t = np.fromfile(path, dtype="<f4").reshape(-1, 3)
+            t1 = time.perf_counter()
+            rec.responses = t
+            t2 = time.perf_counter()
+            del t
+            out["pageable_read_s"] = t1 - t0
+            out["pageable_set_responses_s"] = t2 - t1
+            out["pageable_total_GBps"] = 12 * n / (t2 - t0) / 1e9
+        cli = os.path.join(ROOT, "j-pet-mlem-old_b200", "bin", "2d_strip_reconstruction")
+        if os.access(cli, os.X_OK):
+            img = os.path.join(d, "r.bin")
+            cmd = [cli, path, "-r", repr(GEOM["radius"]), "-l", repr(GEOM["length"]),
+                   "-p", repr(GEOM["p"]), "--n-y-pixels", str(GEOM["n_y"]),
+                   "--n-z-pixels", str(GEOM["n_z"]), "--s-z", repr(GEOM["s_z"]),
+                   "--s-dl", repr(GEOM["s_dl"]), "-i", "1", "-I", str(iters), "-o", img,
+                   "--cuda-device", str(local_rank)]
+            t0 = time.perf_counter()
+            p = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+            wall = time.perf_counter() - t0
+            if p.returncode == 0:
+                out["cli_e2e"] = {
+                    "value": n * iters / wall / 1e6, "unit": UNIT, "wall_s": wall,
+                    "iterations": iters,
+                    "what": "bin/2d_strip_reconstruction <file> -i 1 -I %d -o r.bin: process "
+                            "start, CUDA context, file -> HBM, binning, iterations, image "
+                            "file, wall clock" % iters}
+            else:
+                out["cli_e2e"] = {"error": p.stderr[-300:]}
+    finally:
+        for f in os.listdir(d):
+            os.unlink(os.path.join(d, f))
+        os.rmdir(d)
+    return out
+
+
 def batch_instances(n_inst=64):
     """The batched workload: n_inst reconstructions, instance i seeded by i --
     image n_y x n_z with n in [100, 800], pixel p in {1, 2, 3, 4} mm, strips
@@ -543,6 +609,10 @@ def ours(args, rank, world, local_rank):
             osem["error"] = accuracy_vs_fp64((zu, zd, dl), min(n, args.error_events // 2), 2,
                                              local_rank, n_subsets=8)
 
+    io = None
+    if rank == 0 and world == 1 and not args.no_io:
+        io = io_throughput(zu, zd, dl, local_rank, args.e2e_iters)
+
     batched = None
     achieved_plain = flops_per_iter / (tile_ms / args.steps / 1e3) / 1e12
     if world == 1 and not args.no_batched:
@@ -598,6 +668,8 @@ def ours(args, rank, world, local_rank):
         line["differentiable"] = diff
     if osem is not None:
         line["osem8"] = osem
+    if io is not None:
+        line["io"] = io
     if batched is not None:
         line["batched"] = batched
     if rank == 0 and world == 1 and not args.no_hybrid:
@@ -629,6 +701,7 @@ def main():
     ap.add_argument("--no-differentiable", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-osem", action="store_true")
+    ap.add_argument("--no-io", action="store_true")
     ap.add_argument("--error-events", type=int, default=1_000_000,
                     help="events of the prefix whose 20-iteration image is checked "
                          "against the FP64 oracle (0: no check)")

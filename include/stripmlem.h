@@ -133,6 +133,17 @@ int strip_set_events(strip_ctx* ctx, const float* z_u, const float* z_d,
  * layout and binary event-file layout (response.h:13-20, reconstruction.h:156-167). */
 int strip_set_responses(strip_ctx* ctx, const float* zu_zd_dl, int64_t n,
                         int n_subsets);
+/* Reads events of a binary event file -- raw little-endian binary32 triples
+ * z_u z_d dl, the reference's format (response.h:13-20, read until the end
+ * of the file by reconstruction.h:156-167; a trailing partial triple is
+ * ignored) -- from event `first` on, at most n of them (n < 0: to the end),
+ * straight into device memory, and bins them as strip_set_events.  Several
+ * host threads read chunks into pinned staging buffers while earlier chunks
+ * are being copied to the device.  *n_loaded (may be NULL) receives the
+ * number of events.  Replaces the reference CLI's whole-file read
+ * (reconstruction_cmd.cpp:168-186) for one binary input file. */
+int strip_load_responses_file(strip_ctx* ctx, const char* path, int64_t first,
+                              int64_t n, int n_subsets, int64_t* n_loaded);
 /* Same as strip_set_events with device pointers (already resident in HBM). */
 int strip_set_events_device(strip_ctx* ctx, const float* d_z_u,
                             const float* d_z_d, const float* d_dl, int64_t n,

@@ -181,7 +181,14 @@ int run(int argc, char** argv) {
 
   const bool is_3d = cl.exist("3d-response");
   std::vector<float> zu, zd, dl;
+  // One binary event file with no unit conversion goes from the file to the
+  // device through the library's staged reader (strip_load_responses_file);
+  // everything else is read here first.
+  const bool direct = cl.rest.size() == 1 && ext_of(cl.rest[0]) != ".txt" && !is_3d &&
+                      !cl.exist("scale-length") && !cl.exist("dl-is-time") &&
+                      !cl.exist("dump-responses");
   for (const auto& fn : cl.rest) {
+    if (direct) break;
     if (ext_of(fn) == ".txt") {
       strip_cli::read_events_text(fn, is_3d, zu, zd, dl);
     } else {
@@ -228,8 +235,16 @@ int run(int argc, char** argv) {
 
   Ctx ctx;
   check(nullptr, strip_ctx_create(&g, cl.integer("cuda-device"), &ctx.p), "strip_ctx_create");
-  check(ctx.p, strip_set_events(ctx.p, zu.data(), zd.data(), dl.data(), (int64_t)zu.size(), 1),
-        "strip_set_events");
+  if (direct) {
+    int64_t n_read = 0;
+    check(ctx.p, strip_load_responses_file(ctx.p, cl.rest[0].c_str(), 0, -1, 1, &n_read),
+          "strip_load_responses_file");
+    if (verbose)
+      std::cerr << "# read " << n_read << " responsess from " << cl.rest[0] << std::endl;
+  } else {
+    check(ctx.p, strip_set_events(ctx.p, zu.data(), zd.data(), dl.data(), (int64_t)zu.size(), 1),
+          "strip_set_events");
+  }
   check(ctx.p, strip_set_image(ctx.p, rho.data()), "strip_set_image");
 
   if (gpu) {

@@ -533,6 +533,7 @@ int strip_ctx_destroy(strip_ctx* ctx) {
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   for (cudaEvent_t ev : ctx->tile_marks) cudaEventDestroy(ev);
+  release_staging(ctx);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return STRIP_OK;
@@ -590,15 +591,11 @@ int strip_set_events(strip_ctx* ctx, const float* zu, const float* zd,
   float* dzu = d;
   float* dzd = d + std::max<int64_t>(n, 1);
   float* ddl = d + 2 * std::max<int64_t>(n, 1);
-  cudaError_t e = cudaSuccess;
   if (n > 0) {
-    e = cudaMemcpyAsync(dzu, zu, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dzd, zd, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(ddl, dl, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
-  }
-  if (e != cudaSuccess) {
-    cudaFree(d);
-    CK(e);
+    if (int rc = upload_soa(ctx, zu, zd, dl, n, dzu, dzd, ddl)) {
+      cudaFree(d);
+      return rc;
+    }
   }
   ctx->n_events = n;
   int rc = bin_events(ctx, dzu, dzd, ddl, nullptr, n, n_subsets);
@@ -609,15 +606,12 @@ int strip_set_events(strip_ctx* ctx, const float* zu, const float* zd,
 int strip_set_responses(strip_ctx* ctx, const float* t, int64_t n,
                         int n_subsets) {
   if (!ctx) return STRIP_E_INVALID;
-  if (n < 0 || (n > 0 && !t))
+  if (n < 0 || (n > 0 && !t) || n_subsets < 1 || n_subsets > 4096)
     return fail(ctx, STRIP_E_INVALID, "invalid responses");
-  std::vector<float> zu((size_t)n), zd((size_t)n), dl((size_t)n);
-  for (int64_t i = 0; i < n; ++i) {  // AoS -> SoA, gpu_events_soa.h:18-22
-    zu[i] = t[3 * i];
-    zd[i] = t[3 * i + 1];
-    dl[i] = t[3 * i + 2];
-  }
-  return strip_set_events(ctx, zu.data(), zd.data(), dl.data(), n, n_subsets);
+  if (int rc = set_device(ctx)) return rc;
+  // the triples go to the device as they are; a kernel splits them
+  // (AoS -> SoA, gpu_events_soa.h:18-22)
+  return upload_responses(ctx, t, n, n_subsets);
 }
 
 int strip_set_image(strip_ctx* ctx, const float* rho) {

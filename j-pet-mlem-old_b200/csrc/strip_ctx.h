@@ -50,6 +50,11 @@ struct strip_ctx {
   float* d_item_hist = nullptr;
   unsigned long long* d_fallback = nullptr;  // events rerun in a weighted window
   std::vector<cudaEvent_t> tile_marks;
+  // pinned staging buffers of the host -> device event uploads, one stream
+  // and event each (strip_upload.cu)
+  std::vector<void*> stage_buf;
+  std::vector<cudaStream_t> stage_stream;
+  std::vector<cudaEvent_t> stage_event;
   strip_stats stats{};
   std::string err;
 };
@@ -65,5 +70,14 @@ int ctx_prepare_mlem(strip_ctx* ctx, int mode);
 LaunchArgs ctx_mlem_args(strip_ctx* ctx, int mode);
 // Re-bins the events with `tile` x `tile` pixel tiles.
 int ctx_rebin(strip_ctx* ctx, int tile);
+
+// strip_upload.cu: host arrays to the device through pinned staging buffers
+// filled by several host threads (straight copies for pinned memory).
+// upload_soa copies n floats of each array; upload_responses copies n
+// triples, splits them on the device and bins them (strip_set_events_device).
+int upload_soa(strip_ctx* ctx, const float* zu, const float* zd, const float* dl,
+               int64_t n, float* d_zu, float* d_zd, float* d_dl);
+int upload_responses(strip_ctx* ctx, const float* zu_zd_dl, int64_t n, int n_subsets);
+void release_staging(strip_ctx* ctx);
 
 }  // namespace stripmlem

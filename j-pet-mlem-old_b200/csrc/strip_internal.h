@@ -87,6 +87,10 @@ enum Op {
   OP_GRAD = 3      // d/dsigma of sum_e w_e D_e
 };
 
+// Event triples (z_u, z_d, dl) x n -> three arrays.
+cudaError_t launch_split_triples(const float* aos, int64_t n, float* zu, float* zd,
+                                 float* dl, cudaStream_t st);
+
 struct LaunchArgs {
   ScannerF s;
   KernelF k;          // kernel constants (model sigmas)

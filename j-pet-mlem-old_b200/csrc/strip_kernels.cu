@@ -990,6 +990,17 @@ __global__ void __launch_bounds__(kThreads) k_global(LaunchArgs a) {
   }
 }
 
+__global__ void k_split_triples(const float* __restrict__ aos, int64_t n,
+                                float* __restrict__ zu, float* __restrict__ zd,
+                                float* __restrict__ dl) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    zu[i] = aos[3 * i];
+    zd[i] = aos[3 * i + 1];
+    dl[i] = aos[3 * i + 2];
+  }
+}
+
 __global__ void k_event_boxes(ScannerF s, const float* zu, const float* zd,
                               const float* dl, int64_t n, int4* boxes,
                               int* max_wh, unsigned long long* n_empty) {
@@ -1393,6 +1404,13 @@ cudaError_t launch_update_batch(const BatchUpdateArgs& u, int64_t max_pix,
   if (u.n <= 0) return cudaSuccess;
   const int gx = (int)std::min<int64_t>(std::max<int64_t>((max_pix + kThreads - 1) / kThreads, 1), 64);
   k_update_batch<<<dim3(gx, u.n), kThreads, 0, st>>>(u);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_split_triples(const float* aos, int64_t n, float* zu, float* zd,
+                                 float* dl, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  k_split_triples<<<grid_for(n), kThreads, 0, st>>>(aos, n, zu, zd, dl);
   return cudaGetLastError();
 }
 

@@ -14,6 +14,7 @@ Everything calls the C ABI of lib/libstripmlem.so (include/stripmlem.h); the
 arithmetic runs in the library's sm_100a kernels.  Errors raise StripError.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -242,6 +243,18 @@ class Reconstruction:
 
     def set_schedule(self, tile=32, grab=32):
         self._check(self.lib.strip_set_schedule(self._ctx, int(tile), int(grab)))
+
+    def load_responses_file(self, path, first=0, n=-1, n_subsets=1):
+        """Reads a binary event file (raw f32 triples z_u z_d dl) straight to
+        the device and bins the events (strip_load_responses_file); returns
+        the number of events read."""
+        got = ctypes.c_int64()
+        self._check(self.lib.strip_load_responses_file(
+            self._ctx, os.fsencode(os.fspath(path)), int(first), int(n), int(n_subsets),
+            ctypes.byref(got)))
+        self.n_events = got.value
+        self.n_subsets = int(n_subsets)
+        return got.value
 
     def set_item_events(self, max_events=0):
         """Largest tile work item in events (1..8000), or 0 to let each

@@ -168,6 +168,9 @@ SIGNATURES = {
     "strip_autotune": (ctypes.c_int, [_ctx, ctypes.c_int, _P(Tuning)]),
     "strip_set_schedule": (ctypes.c_int, [_ctx, ctypes.c_int, ctypes.c_int]),
     "strip_set_item_events": (ctypes.c_int, [_ctx, ctypes.c_int]),
+    "strip_load_responses_file": (ctypes.c_int, [_ctx, ctypes.c_char_p, ctypes.c_int64,
+                                                 ctypes.c_int64, ctypes.c_int,
+                                                 _P(ctypes.c_int64)]),
     "strip_debug_pixel_sets": (
         ctypes.c_int,
         [_ctx, _f, _f, _f, ctypes.c_int64, _P(ctypes.c_int32), _P(ctypes.c_int32), _P(ctypes.c_uint64)],

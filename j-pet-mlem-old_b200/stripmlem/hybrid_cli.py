@@ -94,7 +94,7 @@ def lor_segments(centers):
     return seg
 
 
-def naive_image(kept, resp, n, n_planes, p, z_left, segments):
+def naive_image(kept, resp, nc, nr, n_planes, p, llx, lly, z_left, segments):
     """Reconstruction::naive (reconstruction.h:394-405): the count of kept
     events per voxel of their point (the LOR's mid point + up along it, z =
     right), binary32 as the reference computes it.  kept: the kept responses'
@@ -115,12 +115,12 @@ def naive_image(kept, resp, n, n_planes, p, z_left, segments):
     right = f32(0.5) * (zu + zd + (f32(2) * up * tan))
     x = mid[:, 0] + d[:, 0] * up
     y = mid[:, 1] + d[:, 1] * up
-    llx = -f32(p) * f32(n) / f32(2)
-    ix = np.floor((x - llx) / f32(p)).astype(np.int64)
-    iy = np.floor((y - llx) / f32(p)).astype(np.int64)
+    # PixelGrid::pixel_at (pixel_grid.h:59-62) on the grid's lower-left corner
+    ix = np.floor((x - f32(llx)) / f32(p)).astype(np.int64)
+    iy = np.floor((y - f32(lly)) / f32(p)).astype(np.int64)
     iz = np.floor((right - f32(z_left)) / f32(p)).astype(np.int64)
-    ok = (ix >= 0) & (ix < n) & (iy >= 0) & (iy < n) & (iz >= 0) & (iz < n_planes)
-    img = np.zeros((n_planes, n, n), np.int32)
+    ok = (ix >= 0) & (ix < nc) & (iy >= 0) & (iy < nr) & (iz >= 0) & (iz < n_planes)
+    img = np.zeros((n_planes, nr, nc), np.int32)
     np.add.at(img, (iz[ok], iy[ok], ix[ok]), 1)
     return img
 
@@ -131,26 +131,35 @@ def main(argv=None):
     inactive = _ints(a.inactive) if a.inactive else None
     geom = None
     if a.geometry:
-        # run_with_geometry (reconstruction_cmd.cpp:281-363): the grid from the
-        # file, the weights from the matrix
+        # run_with_geometry (reconstruction_cmd.cpp:281-363): the pixel grid
+        # (size and lower-left corner) from the file, the weights from the
+        # matrix; --s-pixel (default: the file's pixel size) only sets the
+        # default z_left, as there
+        if "," in a.system:
+            raise SystemExit("per-plane system matrices (a comma-separated --system list) "
+                             "are not supported; give one matrix")
         geom = hy.read_geometry(a.geometry)
         nc, nr, gp, llx, lly = geom["grid"]
         if abs(llx + gp * nc / 2) > 1e-6 * gp or abs(lly + gp * nr / 2) > 1e-6 * gp:
-            raise SystemExit("the geometry's pixel grid must be centred on the origin")
+            raise SystemExit("the geometry's pixel grid must be centred on the origin "
+                             f"(lower left {llx}, {lly} for {nc} x {nr} pixels of {gp})")
         n = a.n_pixels or max(nc, nr)
         if a.s_pixel is None:
             a.s_pixel = gp
+        p_grid = gp
     else:
         if a.s_pixel is None or a.detector_file is None:
             raise SystemExit("--s-pixel and --detector-file are required with --system")
         n = a.n_pixels or m.n_pixels_in_row
         nc = nr = n
+        p_grid = a.s_pixel
+        llx = lly = -p_grid * n / 2
     n_planes = a.n_planes if a.n_planes is not None else n
     z_left = a.z_left if a.z_left is not None else -n_planes * a.s_pixel / 2
     if a.verbose:
         print(f"3D hybrid reconstruction:\n    detectors = {m.n_detectors}", file=sys.stderr)
-        print(f"   pixel grid = {nc} x {nr} / {a.s_pixel}", file=sys.stderr)
-    rec = hy.HybridReconstruction(nc, nr, n_planes, a.s_pixel, z_left, a.length, a.s_z, a.s_dl,
+        print(f"   pixel grid = {nc} x {nr} / {p_grid}", file=sys.stderr)
+    rec = hy.HybridReconstruction(nc, nr, n_planes, p_grid, z_left, a.length, a.s_z, a.s_dl,
                                   device=a.cuda_device)
     if geom is not None:
         soa = hy.geometry_soa_from_file(geom, m)
@@ -187,8 +196,9 @@ def main(argv=None):
     out_base, out_ext = os.path.splitext(a.output) if a.output else (None, None)
     dims = (nc, nr, n_planes)
     if out_base:
-        _write_map(out_base, out_ext, naive_image(rec.frames()["index"], resp, nc, n_planes,
-                                                  a.s_pixel, z_left, segments), dims, "int")
+        _write_map(out_base, out_ext,
+                   naive_image(rec.frames()["index"], resp, nc, nr, n_planes, p_grid, llx, lly,
+                               z_left, segments), dims, "int")
     n_total = a.blocks * a.iterations
     digits = len(str(n_total)) if n_total > 0 else 1
     for block in range(a.blocks):

@@ -194,9 +194,30 @@ def test_cli_naive_image_matches_reference(case, kw):
     z, cfg, m, resp, centers = golden_inputs()
     n, n_planes, p, z_left = cfg[0], cfg[1], cfg[2], cfg[3]
     res = oh.reconstruct(oracle_setup(cfg), centers, m, resp, 0, **kw)
-    img = hybrid_cli.naive_image(np.flatnonzero(res["keep"]), resp, n, n_planes, p, z_left,
-                                 hybrid_cli.lor_segments(centers))
+    ll = -p * n / 2
+    img = hybrid_cli.naive_image(np.flatnonzero(res["keep"]), resp, n, n, n_planes, p, ll, ll,
+                                 z_left, hybrid_cli.lor_segments(centers))
     assert np.array_equal(img, z[f"{case}_naive"])
+
+
+def test_cli_naive_image_non_square_grid():
+    """A grid of nc != nr (the --geometry path): x bins by columns, y by
+    rows, each from its own lower-left coordinate; the image is
+    (n_planes, nr, nc).  Cropping the golden square grid to fewer rows keeps
+    every count of the rows inside and drops the rest."""
+    from oracle import hybrid as oh
+    from stripmlem import hybrid_cli
+    z, cfg, m, resp, centers = golden_inputs()
+    n, n_planes, p, z_left = cfg[0], cfg[1], cfg[2], cfg[3]
+    res = oh.reconstruct(oracle_setup(cfg), centers, m, resp, 0)
+    kept = np.flatnonzero(res["keep"])
+    segs = hybrid_cli.lor_segments(centers)
+    ll = -p * n / 2
+    full = hybrid_cli.naive_image(kept, resp, n, n, n_planes, p, ll, ll, z_left, segs)
+    r0, nr = 5, n - 9  # rows [5, n - 4): lower-left y moves up by 5 pixels
+    crop = hybrid_cli.naive_image(kept, resp, n, nr, n_planes, p, ll, ll + r0 * p, z_left, segs)
+    assert crop.shape == (n_planes, nr, n)
+    assert np.array_equal(crop, full[:, r0:r0 + nr, :])
 
 
 def test_cli_writes_reference_file_layout(tmp_path):
