@@ -191,6 +191,20 @@ int hybrid_get_image(hybrid_ctx* ctx, float* rho);
 
 int hybrid_get_stats(hybrid_ctx* ctx, hybrid_stats* out);
 
+/* Text responses "first second z_up z_dn dl", one per '\n'-terminated line
+ * (an unterminated last line is not read), parsed with the arithmetic of the
+ * reference's fast text parser (util::text_parser, text_parser.h:82-175, as
+ * Reconstruction::fast_load_txt_events uses it, reconstruction.h:163-186) so
+ * the binary32 values are the reference's; the detector indices keep their
+ * low 16 bits as the reference's short fields do.  `text` holds `length`
+ * bytes; up to `capacity` lines are stored and *n_lines receives the number
+ * of complete lines (call with capacity 0 to count them).  On a malformed
+ * number returns STRIP_E_INVALID with *n_lines = the line's index.  Host
+ * only. */
+int hybrid_parse_responses_text(const char* text, int64_t length, int64_t capacity,
+                                int16_t* first, int16_t* second, float* z_up, float* z_dn,
+                                float* dl, int64_t* n_lines);
+
 /* Test hook: evaluates, on CUDA device `device`, the arctangent the MLEM
  * kernel uses for the strip frame's angular sensitivity (which = 0: atan2(a, b)
  * for a > 0 by an odd degree-15 polynomial) or CUDA's atan2f (which = 1) on

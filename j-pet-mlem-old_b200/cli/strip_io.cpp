@@ -1,5 +1,7 @@
 #include "strip_io.h"
 
+#include "text_parse.h"
+
 #include <fcntl.h>
 #include <unistd.h>
 
@@ -42,84 +44,16 @@ void read_events_binary(const std::string& path, std::vector<float>& z_u,
 
 namespace {
 
-// Integer part as the reference's parse_integer: int accumulation that wraps
-// on overflow (the reference's signed arithmetic, as GCC compiles it).
-int parse_digits(const char*& p, int& n_digits) {
-  n_digits = 0;
-  uint32_t sum = 0;
-  while (*p >= '0' && *p <= '9') {
-    sum = sum * 10u + (uint32_t)(*p - '0');
-    ++p;
-    ++n_digits;
-  }
-  return (int32_t)sum;
-}
-
-int parse_sign(const char*& p) {
-  if (*p == '-') {
-    ++p;
-    return -1;
-  }
-  if (*p == '+') ++p;
-  return 1;
-}
-
-constexpr int kMaxExponent = 300;
-
-// 0.1^e built as 0.1f * 0.1^(e-1) in binary32, and the reference's positive
-// powers, 10 * 0.1^(e-1) (text_parser.h:82-100: only e <= 1 is a true power
-// of ten).
-float pow10_neg(int e) {
-  static std::array<float, kMaxExponent + 1> cache = [] {
-    std::array<float, kMaxExponent + 1> c{};
-    c[0] = 1.0f;
-    for (int i = 1; i <= kMaxExponent; ++i) c[i] = 0.1f * c[i - 1];
-    return c;
-  }();
-  return cache[e];
-}
-float pow10_pos(int e) { return e == 0 ? 1.0f : 10.0f * pow10_neg(e - 1); }
-
-int parse_int_field(const char*& p) {
-  while (*p == ' ') ++p;
-  const int sign = parse_sign(p);
-  int nd;
-  return sign * parse_digits(p, nd);
-}
+int parse_int_field(const char*& p) { return striptext::parse_int(p); }
 
 }  // namespace
 
+// The reference fast parser's arithmetic lives in the library (text_parse.h).
 float parse_fp_reference(const char*& p) {
-  while (*p == ' ') ++p;  // skip_space: blanks only
-  int n_whole;
-  const int sign = parse_sign(p);
-  const int whole = parse_digits(p, n_whole);
-  float val = (float)whole;
-  if (*p == '.') {
-    ++p;
-    int n_frac = 0;
-    const int frac = parse_digits(p, n_frac);
-    if (n_whole == 0 && n_frac == 0)
-      throw std::string("period with no digits either before or after");
-    if (n_frac > 0) {
-      const float scaled = (float)frac * pow10_neg(std::min(n_frac, kMaxExponent));
-      val = val + scaled;
-    }
-  } else if (n_whole == 0) {
-    throw std::string("neither whole part nor period");
-  }
-  if (*p == 'e' || *p == 'E') {
-    ++p;
-    int n_exp;
-    const int esign = parse_sign(p);
-    const int e = esign * parse_digits(p, n_exp);
-    if (n_exp == 0) throw std::string("found exponent char but no exponent");
-    if (e > kMaxExponent || e < -kMaxExponent)
-      throw std::string("exponent out of range");
-    if (e > 0) val = val * pow10_pos(e);
-    else if (e < 0) val = val * pow10_neg(-e);
-  }
-  return val * (float)sign;
+  float v = 0.0f;
+  const char* err = nullptr;
+  if (!striptext::parse_fp(p, v, &err)) throw std::string(err);
+  return v;
 }
 
 void read_events_text(const std::string& path, bool is_3d,

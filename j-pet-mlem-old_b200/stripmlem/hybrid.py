@@ -243,96 +243,23 @@ def write_responses(path, first, second, z_up, z_dn, dl):
     r.tofile(path)
 
 
-_F32 = np.float32
-_POW10_NEG = [_F32(1.0)]
-for _i in range(300):
-    _POW10_NEG.append(_F32(_F32(0.1) * _POW10_NEG[-1]))
-
-
-class _TextParser:
-    """util::text_parser (src/util/text_parser.h) as the reference's fast
-    loader uses it: blanks skipped, int accumulation that wraps, binary32
-    value = whole + frac * 0.1^n_frac (0.1^n built as 0.1 * 0.1^(n-1)),
-    exponents by 10 * 0.1^(e-1) or 0.1^e, the sign applied last."""
-
-    def __init__(self, line):
-        self.s = line
-        self.i = 0
-
-    def _skip(self):
-        while self.i < len(self.s) and self.s[self.i] == " ":
-            self.i += 1
-
-    def _sign(self):
-        if self.i < len(self.s) and self.s[self.i] in "+-":
-            self.i += 1
-            return -1 if self.s[self.i - 1] == "-" else 1
-        return 1
-
-    def _digits(self):
-        v = 0
-        n = 0
-        while self.i < len(self.s) and "0" <= self.s[self.i] <= "9":
-            v = (v * 10 + ord(self.s[self.i]) - 48) & 0xFFFFFFFF
-            self.i += 1
-            n += 1
-        return (v - (1 << 32) if v >= 1 << 31 else v), n
-
-    def int_(self):
-        self._skip()
-        sign = self._sign()
-        v, _ = self._digits()
-        return sign * v
-
-    def float_(self):
-        self._skip()
-        sign = self._sign()
-        whole, n_whole = self._digits()
-        val = _F32(whole)
-        if self.i < len(self.s) and self.s[self.i] == ".":
-            self.i += 1
-            frac, n_frac = self._digits()
-            if n_whole == 0 and n_frac == 0:
-                raise ValueError("period with no digits either before or after")
-            if n_frac > 0:
-                val = _F32(val + _F32(_F32(frac) * _POW10_NEG[min(n_frac, 300)]))
-        elif n_whole == 0:
-            raise ValueError("neither whole part nor period")
-        if self.i < len(self.s) and self.s[self.i] in "eE":
-            self.i += 1
-            esign = self._sign()
-            e, n_exp = self._digits()
-            e *= esign
-            if n_exp == 0:
-                raise ValueError("found exponent char but no exponent")
-            if e > 300 or e < -300:
-                raise ValueError("exponent out of range")
-            if e > 0:
-                val = _F32(val * _F32(_F32(10.0) * _POW10_NEG[e - 1]))
-            elif e < 0:
-                val = _F32(val * _POW10_NEG[-e])
-        return _F32(val * _F32(sign))
-
-
 def read_responses_text(path):
     """Text responses `first second z_up z_dn dl` parsed as the reference's
     fast loader parses them (fast_load_txt_events, reconstruction.h:163-186,
-    util::text_parser::read_lines: a line counts when it ends in a newline)."""
-    data = open(path, "rb").read().decode("ascii")
-    lines = data.split("\n")[:-1]
-    n = len(lines)
+    util::text_parser::read_lines: a line counts when it ends in a newline),
+    by the library's parser (hybrid_parse_responses_text)."""
+    data = open(path, "rb").read()
+    n = data.count(b"\n")
     first = np.empty(n, np.int16)
     second = np.empty(n, np.int16)
     zu = np.empty(n, np.float32)
     zd = np.empty(n, np.float32)
     dl = np.empty(n, np.float32)
-    for k, line in enumerate(lines):
-        p = _TextParser(line)
-        first[k] = np.array(p.int_()).astype(np.int16)
-        second[k] = np.array(p.int_()).astype(np.int16)
-        zu[k] = p.float_()
-        zd[k] = p.float_()
-        dl[k] = p.float_()
+    got = ctypes.c_int64()
+    rc = _lib.load().hybrid_parse_responses_text(data, len(data), n, _vp(first), _vp(second),
+                                                 _vp(zu), _vp(zd), _vp(dl), ctypes.byref(got))
+    if rc != _lib.STRIP_OK:
+        raise ValueError(f"{path}: malformed number on line {got.value + 1}")
     return first, second, zu, zd, dl
 
 

@@ -237,9 +237,10 @@ def test_cli_writes_reference_file_layout(tmp_path):
 
 
 def test_text_responses_parse_as_the_reference(tmp_path):
-    """Text responses (mixed number formats) read by stripmlem.hybrid's port
-    of the reference's fast text parser reproduce the reference's image
-    from the same file bit for bit through the oracle."""
+    """Text responses (mixed number formats) read by the library's statement
+    of the reference's fast text parser (hybrid_parse_responses_text)
+    reproduce the reference's image from the same file bit for bit through
+    the oracle."""
     from oracle import hybrid as oh
     from stripmlem import hybrid as hy
     z, cfg, m, resp, centers = golden_inputs()
@@ -251,6 +252,18 @@ def test_text_responses_parse_as_the_reference(tmp_path):
     assert np.array_equal(res["rho"], z["text_rho"])
     st = res["stats"]
     assert [st["used_events"], st["used_pixels"], st["used_voxels"]] == list(z["text_counts"])
+
+
+def test_text_responses_malformed_line_reported(tmp_path):
+    from stripmlem import hybrid as hy
+    path = tmp_path / "bad.txt"
+    path.write_text("1 0 1.5 -2 30\n3 2 1e2 . 4\n")
+    with pytest.raises(ValueError, match="line 2"):
+        hy.read_responses(str(path))
+    path.write_text("70000 -1 1.5 -2 30\n4 3 2 1 0")  # last line unterminated
+    f, s_, zu, zd, dl = hy.read_responses(str(path))
+    assert len(f) == 1 and f[0] == np.int16(70000 - 65536) and s_[0] == -1
+    assert zu[0] == np.float32(1.5) and dl[0] == np.float32(30)
 
 
 def test_geometry_file_path_reproduces_reference(tmp_path):
