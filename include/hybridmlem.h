@@ -205,6 +205,15 @@ int hybrid_parse_responses_text(const char* text, int64_t length, int64_t capaci
                                 int16_t* first, int16_t* second, float* z_up, float* z_dn,
                                 float* dl, int64_t* n_lines);
 
+/* Adds the converter's Gaussian errors to n converted responses in place:
+ * for each response in order, z_up += N(0, sigma_z), z_dn += N(0, sigma_z),
+ * dl += N(0, sigma_dl), drawn from std::normal_distribution<double> (one
+ * for z, one for dl) over one std::mt19937_64(seed) -- 3d_tool_convert
+ * --warsaw's smearing (src/3d/tool/convert_cmd.cpp:92-95,149-151), value for
+ * value with the same C++ standard library.  Host only. */
+int hybrid_smear_responses(int64_t seed, double sigma_z, double sigma_dl, int64_t n,
+                           double* z_up, double* z_dn, double* dl);
+
 /* Test hook: evaluates, on CUDA device `device`, the arctangent the MLEM
  * kernel uses for the strip frame's angular sensitivity (which = 0: atan2(a, b)
  * for a > 0 by an odd degree-15 polynomial) or CUDA's atan2f (which = 1) on

@@ -286,6 +286,8 @@ SIGNATURES.update({
     "hybrid_get_stats": (ctypes.c_int, [_ctx, _P(HybridStats)]),
     "hybrid_debug_atan2": (ctypes.c_int, [ctypes.c_int32, _vp, _vp, ctypes.c_int64,
                                           ctypes.c_int32, _vp]),
+    "hybrid_smear_responses": (ctypes.c_int, [ctypes.c_int64, ctypes.c_double, ctypes.c_double,
+                                              ctypes.c_int64, _vp, _vp, _vp]),
     "hybrid_parse_responses_text": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int64,
                                                    ctypes.c_int64] + [_vp] * 5
                                     + [_P(ctypes.c_int64)]),

@@ -508,9 +508,9 @@ def convert_warsaw(lines, polygons, length, sigma_z=0.0, sigma_dl=0.0, seed=0, o
     Pairs with |z| > length / 2 are skipped, as are pairs whose scatter
     differs from `only` (when only != 0) and points inside no detector
     (Polygon::contains with tolerance 1e-4); the larger detector index comes
-    first.  With sigma_z = sigma_dl = 0 the output is the reference's exactly;
-    otherwise the Gaussian errors come from numpy's generator, not the
-    reference's std::mt19937_64."""
+    first.  The Gaussian errors (sigma_z on z, sigma_dl on dl) are the
+    reference's for the same seed: std::normal_distribution over
+    std::mt19937_64 in output order (hybrid_smear_responses)."""
     rows = [ln.split() for ln in lines if ln.strip()]
     if not rows:
         z = np.zeros(0)
@@ -537,13 +537,14 @@ def convert_warsaw(lines, polygons, length, sigma_z=0.0, sigma_dl=0.0, seed=0, o
     d1, d2 = np.where(sw, d2, d1), np.where(sw, d1, d2)
     z1, z2 = np.where(sw, z2, z1), np.where(sw, z1, z2)
     t1, t2 = np.where(sw, t2, t1), np.where(sw, t1, t2)
-    dl = (t1 - t2) * _C_PS
-    rng = np.random.default_rng(seed)
-    n = len(d1)
-    ez1 = rng.normal(0, sigma_z, n) if sigma_z > 0 else 0.0
-    ez2 = rng.normal(0, sigma_z, n) if sigma_z > 0 else 0.0
-    edl = rng.normal(0, sigma_dl, n) if sigma_dl > 0 else 0.0
-    return (d1.astype(np.int16), d2.astype(np.int16), z1 * _CM + ez1, z2 * _CM + ez2, dl + edl)
+    dl = np.ascontiguousarray((t1 - t2) * _C_PS)
+    zu = np.ascontiguousarray(z1 * _CM)
+    zd = np.ascontiguousarray(z2 * _CM)
+    rc = _lib.load().hybrid_smear_responses(int(seed), float(sigma_z), float(sigma_dl), len(d1),
+                                            _vp(zu), _vp(zd), _vp(dl))
+    if rc != _lib.STRIP_OK:
+        raise HybridError(rc, "hybrid_smear_responses")
+    return d1.astype(np.int16), d2.astype(np.int16), zu, zd, dl
 
 
 def convert_tbednarski(lines, relative_time=False):

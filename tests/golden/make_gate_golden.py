@@ -10,8 +10,9 @@ Inputs (seeded synthetic, in the GATE text layouts the converter reads):
               detectors, |z| beyond the barrel, scatter flags 0..3
   tbednarski  300 records `du dd t_ul t_ur t_dl t_dr` (detectors from 1, ps)
 Outputs, the reference's stdout parsed as numbers (it prints 6 significant
-digits): warsaw with --s-z 0 --s-dl 0 (all pairs, and --only 1),
-tbednarski default and --relative-time.
+digits): warsaw with --s-z 0 --s-dl 0 (all pairs, and --only 1) and with
+--s-z 0.01 --s-dl 0.05 --seed 5 (smeared), tbednarski default and
+--relative-time.
 """
 import os
 import subprocess
@@ -82,6 +83,8 @@ def main():
             "warsaw_all": run(SCANNER + ["--warsaw", "--s-z", "0", "--s-dl", "0"], w, tmp),
             "warsaw_only1": run(SCANNER + ["--warsaw", "--s-z", "0", "--s-dl", "0",
                                            "--only", "1"], w, tmp),
+            "warsaw_smeared": run(SCANNER + ["--warsaw", "--s-z", "0.01", "--s-dl", "0.05",
+                                             "--seed", "5"], w, tmp),
             "tbednarski": run(SCANNER + ["--tbednarski"], t, tmp),
             "tbednarski_rel": run(SCANNER + ["--tbednarski", "--relative-time"], t, tmp),
         }

@@ -1,8 +1,8 @@
 """GATE text converters (3d_tool_convert, src/3d/tool/convert_cmd.cpp) of
 stripmlem.hybrid against the reference binary's own output, committed in
 tests/golden/gate_small.npz (made by tests/golden/make_gate_golden.py).
-Detector pairs exactly; values to the 6 significant digits the reference
-prints.  CPU only."""
+Detector pairs exactly; values, the smeared ones included, to the 6
+significant digits the reference prints.  CPU only."""
 import os
 
 import numpy as np
@@ -38,6 +38,24 @@ def test_tbednarski_matches_reference(key, rel):
     assert got.shape == ref.shape
     assert np.array_equal(got[:, :2], ref[:, :2])
     assert np.allclose(got[:, 2:], ref[:, 2:], rtol=1e-5, atol=1e-6)
+
+
+def test_warsaw_smearing_matches_reference():
+    """With --s-z 0.01 --s-dl 0.05 --seed 5 the smeared values are the
+    reference's (std::normal_distribution over std::mt19937_64, drawn in
+    output order), to the 6 digits it prints."""
+    from stripmlem import hybrid as hy
+    z = np.load(GOLDEN)
+    got = as_table(hy.convert_warsaw(list(z["warsaw_in"]), hy.Barrel().polygons, 0.5,
+                                     sigma_z=0.01, sigma_dl=0.05, seed=5))
+    ref = z["warsaw_smeared"]
+    assert got.shape == ref.shape
+    assert np.array_equal(got[:, :2], ref[:, :2])
+    assert np.allclose(got[:, 2:], ref[:, 2:], rtol=1e-5, atol=1e-9)
+    # a different seed gives other errors
+    other = as_table(hy.convert_warsaw(list(z["warsaw_in"]), hy.Barrel().polygons, 0.5,
+                                       sigma_z=0.01, sigma_dl=0.05, seed=6))
+    assert not np.allclose(other[:, 2:], ref[:, 2:], rtol=1e-5, atol=1e-9)
 
 
 def test_warsaw_smearing_and_empty_input():
