@@ -23,7 +23,9 @@ oracle/strip_oracle.c):
               sets (what the 1e-4 parity bar is stated against)
 Errors: rel_l2 = |x - x64| / |x64|; max_abs_rel_peak = max |x - x64| /
 max x64; max_rel_1pct = max |x - x64| / x64 over pixels above 1 % of the
-peak.
+peak.  table_vs_f64_sets32 holds the same against oracle_f64_sets32, and
+mode_spread_rel_l2 the largest rel-L2 between gpu_fp32 / gpu_kahan and
+gpu_fp64.
 """
 import json
 import os
@@ -118,13 +120,22 @@ def run(args, local_rank, host_cores):
         cols["reference"] = ref_imgs
     table = {name: {str(it): errors(imgs[it], ref64[it]) for it in CHECKPOINTS if it in imgs}
              for name, imgs in cols.items()}
+    # against the FP64 oracle with the reference's binary32 sets (the parity bar's reference),
+    # and the spread between the three GPU accumulation modes
+    sets32 = cols["oracle_f64_sets32"]
+    table_sets32 = {name: {str(it): errors(imgs[it], sets32[it]) for it in CHECKPOINTS
+                           if it in imgs}
+                    for name, imgs in cols.items() if name != "oracle_f64_sets32"}
+    spread = {str(it): max(errors(cols[a][it], cols["gpu_fp64"][it])["rel_l2"]
+                           for a in ("gpu_fp32", "gpu_kahan")) for it in CHECKPOINTS}
     line = {"metric": "strip MLEM image error vs the full-FP64 oracle", "path": "precision",
             "config": {"workload": "strip MLEM, 250x200 image of 2 mm pixels, R=200 mm, "
                                    "L=500 mm, sigma_z=10 mm, sigma_dl=42 mm, 3-ellipse phantom",
                        "events": n, "seed": SEED,
                        "sample": f"first {n} events of the 5e7-event stream",
                        "iterations": list(CHECKPOINTS)},
-            "data": "synthetic", "table": table,
+            "data": "synthetic", "table": table, "table_vs_f64_sets32": table_sets32,
+            "mode_spread_rel_l2": spread,
             "oracle_full_fp64_s": t64, "reference_s": ref_s,
             "reference_threads": cores if ref_imgs is not None else None}
     print(json.dumps(line), flush=True)
