@@ -46,7 +46,7 @@ int ensure_staging(strip_ctx* ctx) {
     void* b = nullptr;
     cudaStream_t s = nullptr;
     cudaEvent_t e = nullptr;
-    if (cudaHostAlloc(&b, kStageBytes, cudaHostAllocDefault) != cudaSuccess ||
+    if (cudaHostAlloc(&b, kStageBytes, cudaHostAllocPortable) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
       if (b) cudaFreeHost(b);
