@@ -197,8 +197,14 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
         if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc = STRIP_E_CUDA;
       if (rc != STRIP_OK) break;
       // capture one step as a graph (kernel attributes are set beforehand)
-      if (tile_batch_reserve_smem(b->mode, b->accum,
-                                  std::max(b->cls_smem[0], b->cls_smem[1])) != cudaSuccess ||
+      // (each class has its own kernel: 512-thread CTAs for the narrow
+      // windows, 1024-thread CTAs for the wide ones)
+      bool attr_ok = true;
+      for (int c = 0; c < 2; ++c)
+        if (b->cls_count[c] > 0 &&
+            tile_batch_reserve_smem(b->mode, b->accum, b->cls_smem[c]) != cudaSuccess)
+          attr_ok = false;
+      if (!attr_ok ||
           cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         rc = STRIP_E_CUDA;
         break;

@@ -35,6 +35,11 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
+// Tile kernels whose shared-memory windows leave room for one CTA per SM
+// run 1024-thread CTAs (32 warps, 64 registers each), so the SM keeps as
+// many resident warps as with two 512-thread CTAs.
+constexpr int kWideThreads = 1024;
+constexpr int kMaxWarps = kWideThreads / 32;
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -680,7 +685,7 @@ __device__ __forceinline__ RowTables warp_tables(char* base, int cap, int warp) 
 // and |w_e| <= W, the item's largest weight, so with B = kbound * W the
 // scale 2^s keeps each addend below 2^22 and the item's sum below 2^31.
 __device__ int adjoint_shift(const LaunchArgs& a, const WorkItem& it, int lane) {
-  __shared__ float s_wmax[kWarps];
+  __shared__ float s_wmax[kMaxWarps];
   __shared__ int s_shift;
   float m = 0.0f;
   for (int64_t i = it.begin + threadIdx.x; i < it.begin + it.count;
@@ -755,7 +760,7 @@ __device__ __forceinline__ void run_item(const LaunchArgs& a, const WorkItem& it
 
 // Sum of v over the CTA, returned to every thread (two barriers).
 __device__ __forceinline__ float block_sum(float v) {
-  __shared__ float s_part[kWarps];
+  __shared__ float s_part[kMaxWarps];
   __shared__ float s_total;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
@@ -918,8 +923,10 @@ constexpr int tile_ctas_per_sm() {
 template <int OP>
 constexpr int tile_windows() { return OP == OP_MLEM ? 2 : 1; }
 
-template <int OP, int MODE, int ACC>
-__global__ void __launch_bounds__(kThreads, tile_ctas_per_sm<OP, MODE>())
+template <int OP, int MODE, int ACC, int THREADS>
+__global__ void __launch_bounds__(THREADS, THREADS == kWideThreads
+                                               ? 1
+                                               : tile_ctas_per_sm<OP, MODE>())
     k_tile(const __grid_constant__ LaunchArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   __shared__ int s_next_group;
@@ -930,8 +937,8 @@ __global__ void __launch_bounds__(kThreads, tile_ctas_per_sm<OP, MODE>())
 // Persistent tile kernel over the work items of several reconstructions: a
 // CTA takes item after item from a global counter; item i belongs to member
 // items[i].member, whose arguments live in the kernel's parameter space.
-template <int MODE, int ACC>
-__global__ void __launch_bounds__(kThreads, 2)
+template <int MODE, int ACC, int THREADS>
+__global__ void __launch_bounds__(THREADS, THREADS == kWideThreads ? 1 : 2)
     k_tile_batch(const __grid_constant__ BatchArgs b, const BatchItem* items,
                  int n_items, int* counter) {
   extern __shared__ __align__(16) char smem_raw[];
@@ -1294,12 +1301,13 @@ constexpr int kSetsCap = 64;
 
 template <int OP, int MODE, int ACC>
 cudaError_t launch_tile_t(const LaunchArgs& a, cudaStream_t st) {
-  auto fn = k_tile<OP, MODE, ACC>;
   const int smem = a.t.smem_bytes / 2 * tile_windows<OP>();
+  const bool wide = smem > kNarrowSmemBytes;  // one CTA per SM: 1024 threads
+  auto fn = wide ? k_tile<OP, MODE, ACC, kWideThreads> : k_tile<OP, MODE, ACC, kThreads>;
   cudaError_t err = cudaFuncSetAttribute(
       fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (err != cudaSuccess) return err;
-  fn<<<a.n_items, kThreads, smem, st>>>(a);
+  fn<<<a.n_items, wide ? kWideThreads : kThreads, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -1367,20 +1375,33 @@ cudaError_t launch_global(int op, int mode, int accum, const LaunchArgs& a,
   }
 }
 
-template <class F>
-cudaError_t with_tile_batch(int mode, int accum, F&& pick) {
+template <int THREADS, class F>
+cudaError_t with_tile_batch_t(int mode, int accum, F&& pick) {
   if (mode == STRIP_MODE_CPU) {
-    if (accum == STRIP_ACCUM_FP32) return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP32>);
-    if (accum == STRIP_ACCUM_FP64) return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP64>);
-    return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_KAHAN>);
+    if (accum == STRIP_ACCUM_FP32)
+      return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP32, THREADS>);
+    if (accum == STRIP_ACCUM_FP64)
+      return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP64, THREADS>);
+    return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_KAHAN, THREADS>);
   }
-  if (accum == STRIP_ACCUM_FP32) return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_FP32>);
-  if (accum == STRIP_ACCUM_FP64) return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_FP64>);
-  return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_KAHAN>);
+  if (accum == STRIP_ACCUM_FP32)
+    return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_FP32, THREADS>);
+  if (accum == STRIP_ACCUM_FP64)
+    return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_FP64, THREADS>);
+  return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_KAHAN, THREADS>);
+}
+
+// The persistent batch kernel of a shared-memory class: windows that fit two
+// CTAs per SM run 512-thread CTAs, wider ones 1024-thread CTAs, one per SM.
+template <class F>
+cudaError_t with_tile_batch(int mode, int accum, int smem_bytes, F&& pick) {
+  if (smem_bytes > kNarrowSmemBytes)
+    return with_tile_batch_t<kWideThreads>(mode, accum, pick);
+  return with_tile_batch_t<kThreads>(mode, accum, pick);
 }
 
 cudaError_t tile_batch_reserve_smem(int mode, int accum, int smem_bytes) {
-  return with_tile_batch(mode, accum, [&](auto fn) {
+  return with_tile_batch(mode, accum, smem_bytes, [&](auto fn) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 smem_bytes);
   });
@@ -1390,12 +1411,13 @@ cudaError_t launch_tile_batch(int mode, int accum, const BatchArgs& b,
                               const BatchItem* items, int n_items, int* counter,
                               int smem_bytes, int sm_count, cudaStream_t st) {
   if (n_items <= 0) return cudaSuccess;
+  const bool wide = smem_bytes > kNarrowSmemBytes;
   auto pick = [&](auto fn) -> cudaError_t {
-    const int grid = std::min(n_items, sm_count * 2);
-    fn<<<grid, kThreads, smem_bytes, st>>>(b, items, n_items, counter);
+    const int grid = std::min(n_items, sm_count * (wide ? 1 : 2));
+    fn<<<grid, wide ? kWideThreads : kThreads, smem_bytes, st>>>(b, items, n_items, counter);
     return cudaGetLastError();
   };
-  return with_tile_batch(mode, accum, pick);
+  return with_tile_batch(mode, accum, smem_bytes, pick);
 }
 
 
