@@ -66,6 +66,29 @@ def test_null_context_calls_rejected(lib):
     assert lib.strip_ctx_destroy(None) == _lib.STRIP_E_INVALID
     assert lib.strip_iterate(None, 1, 0, 1, 0, _lib.PROGRESS_CB(), None) == _lib.STRIP_E_INVALID
     assert lib.strip_set_events(None, None, None, None, 0, 1) == _lib.STRIP_E_INVALID
+    assert lib.strip_load_responses_file(None, b"x.bin", 0, -1, 1, None) == _lib.STRIP_E_INVALID
+    assert lib.strip_set_item_events(None, 8000) == _lib.STRIP_E_INVALID
+
+
+def test_host_only_entry_points_validate_arguments(lib):
+    """The text parser and the converter's smearing run on the host: bad
+    arguments are rejected with a status, no device needed."""
+    import ctypes
+    from stripmlem import _lib
+    n = ctypes.c_int64()
+    assert lib.hybrid_parse_responses_text(None, 0, 0, None, None, None, None, None,
+                                           ctypes.byref(n)) == _lib.STRIP_E_INVALID
+    text = b"1 0 1 2 3\n2 1 4 5 6\n"
+    assert lib.hybrid_parse_responses_text(text, len(text), 0, None, None, None, None, None,
+                                           ctypes.byref(n)) == _lib.STRIP_OK
+    assert n.value == 2  # capacity 0: counting only
+    z = np.zeros(3)
+    assert lib.hybrid_smear_responses(1, -1.0, 1.0, 3, z.ctypes.data, z.ctypes.data,
+                                      z.ctypes.data) == _lib.STRIP_E_INVALID
+    a, b, c = np.zeros(3), np.zeros(3), np.zeros(3)
+    assert lib.hybrid_smear_responses(1, 0.0, 0.0, 3, a.ctypes.data, b.ctypes.data,
+                                      c.ctypes.data) == _lib.STRIP_OK
+    assert not (a.any() or b.any() or c.any())  # zero sigmas leave the values
 
 
 def test_generator_runs_on_host_and_is_deterministic():
