@@ -467,6 +467,24 @@ def batched_throughput(local_rank, n_inst, warmup, steps, autotune=True):
             r.close()
 
 
+def secondary_rates(n_in, tile_ms, clocks, n_sm=148):
+    """The work model's special-function and atomic rates: one ex2 and one
+    scatter-add per in-ellipse pixel and iteration.  The SFU peak is the
+    nominal 16 MUFU results per SM and clock at the sampled SM clock."""
+    per_s = n_in / (tile_ms / 1e3)
+    mhz = clocks.get("sm_mhz") or 1965.0
+    sfu_peak = n_sm * 16 * mhz * 1e6
+    return {
+        "model_ex2_per_s": per_s, "sfu_nominal_peak_per_s": sfu_peak,
+        "sfu_frac": per_s / sfu_peak,
+        "scatter_adds_per_s": per_s,
+        "note": "per the work model (one ex2 and one scatter-add per in-ellipse pixel); "
+                "the kernel evaluates the Gaussian along a run by a two-multiply "
+                "recurrence (one ex2 pair per row) and scatters with one 32-bit "
+                "shared-memory reduction per pixel, flushed to HBM once per work item",
+    }
+
+
 def ours(args, rank, world, local_rank):
     import torch
     import stripmlem as sm
@@ -561,20 +579,31 @@ def ours(args, rank, world, local_rank):
     if args.e2e_steps > 0:
         img = np.empty((GEOM["n_y"], GEOM["n_z"]), np.float32)
         times = []
-        for s in range(args.e2e_steps + 1):
-            if dist is not None:
-                dist.barrier()
-            torch.cuda.synchronize()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record()
-            rec.set_events(zu, zd, dl)
-            rec.rho = np.ones_like(img)
-            iterate(args.e2e_iters)
-            img[...] = rec.rho
-            b.record()
-            torch.cuda.synchronize()
-            if s > 0:
-                times.append(a.elapsed_time(b) / 1e3)
+        # host wall time of each phase (every call returns once its work is
+        # done), summed over the timed steps
+        phases = {"set_events": 0.0, "set_image": 0.0, "iterations": 0.0, "get_image": 0.0}
+        with ClockSampler(local_rank) as clk_e2e:
+            for s in range(args.e2e_steps + 1):
+                if dist is not None:
+                    dist.barrier()
+                torch.cuda.synchronize()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                w0 = time.perf_counter()
+                rec.set_events(zu, zd, dl)
+                w1 = time.perf_counter()
+                rec.rho = np.ones_like(img)
+                w2 = time.perf_counter()
+                iterate(args.e2e_iters)
+                w3 = time.perf_counter()
+                img[...] = rec.rho
+                w4 = time.perf_counter()
+                b.record()
+                torch.cuda.synchronize()
+                if s > 0:
+                    times.append(a.elapsed_time(b) / 1e3)
+                    for k, dt in zip(phases, (w1 - w0, w2 - w1, w3 - w2, w4 - w3)):
+                        phases[k] += dt
         e2e_t = sum(times) / len(times)
         if dist is not None:
             tt = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
@@ -584,6 +613,8 @@ def ours(args, rank, world, local_rank):
                "unit": UNIT, "h2d_bytes_per_step": int(3 * 4 * n),
                "d2h_bytes_per_step": int(img.nbytes), "steps": len(times),
                "iterations_per_step": args.e2e_iters,
+               "phases_s_per_step": {k: v / len(times) for k, v in phases.items()},
+               "clocks": clk_e2e.summary(),
                "timed": "set_events (pinned host -> HBM, binning) + iterations + image D2H, "
                         "CUDA events, max over ranks"}
 
@@ -651,6 +682,7 @@ def ours(args, rank, world, local_rank):
             "bbox_pixels_per_iter": work_bb.value, "ellipse_pixels_per_iter": work_in.value,
             "tile_ms_per_step": tile_ms / args.steps,
             "peak_source": "measured live: strip_probe_fp32_peak (FMA chains, this GPU)",
+            "secondary": secondary_rates(work_in.value, tile_ms / args.steps, clocks),
         },
         "clocks": clocks,
         "gpu_launches": launches,

@@ -65,6 +65,10 @@ void launch_frames(const GridF& g, const GeometryDev& geo, const int16_t* first,
                    cudaStream_t st);
 void launch_compact(const Frame* frames, const int32_t* keep, const int64_t* offs, int64_t n,
                     Frame* out, int64_t* out_index, cudaStream_t st);
+// The frame events in LOR order (stable: response order within a LOR), for
+// the iteration kernel; synchronises the stream.
+cudaError_t order_frames_by_lor(const Frame* frames, int32_t n, int64_t n_lors, Frame* out,
+                                cudaStream_t st);
 
 // hybrid_kernels.cu
 void launch_to_zfast(const GridF& g, const float* rho, float* rho_t, cudaStream_t st);

@@ -21,7 +21,9 @@
 // atan2(u - v, 1 + u v) by atan2_pos below, and an image load.  (A table of
 // 1 / sens per pixel info and plane -- it depends on the LOR, the pixel and
 // the plane only -- was slower: 414 against 252 ms per iteration on the
-// big-barrel workload, the walk waiting on its HBM loads.)  Pass 1 keeps each
+// big-barrel workload, the walk waiting on its HBM loads; with the events in
+// LOR order, so that the rows in use stay in L2, still 279 against 204 ms.)
+// Pass 1 keeps each
 // voxel's weight in a per-warp shared cache (first kCache voxels) and the
 // next kSpill in a per-warp slab of global memory (written and read back by
 // the same warp within microseconds, so it stays in L2); pass 2
@@ -173,8 +175,10 @@ k_mlem(const GridF g, const GeometryDev geo, const float* __restrict__ sens,
   const int wib = threadIdx.x >> 5;
   WarpSmem& sm = reinterpret_cast<WarpSmem*>(smem_raw)[wib];
   float* slab = spill + ((int64_t)blockIdx.x * kWarps + wib) * kSpill;
-  const int64_t n_warps = (int64_t)gridDim.x * kWarps;
   const float half_L = g.L / 2;
+  // grid-stride over the events (in LOR order: the warps resident at one
+  // time work on a few LORs, whose pixel infos and image lines stay in L2)
+  const int64_t n_warps = (int64_t)gridDim.x * kWarps;
   for (int64_t e = (int64_t)blockIdx.x * kWarps + wib; e < n_frames; e += n_warps) {
     const Frame f = frames[e];
     const int n_pix = f.info_end - f.info_begin;

@@ -3,6 +3,7 @@
 // is compiled with -fmad=false: every binary32 operation of the frame
 // translation rounds where the reference's C++ says, so the pixel-info and
 // plane ranges of each event equal the reference's bit for bit.
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include "hybrid_internal.h"
@@ -181,6 +182,51 @@ void launch_frames(const GridF& g, const GeometryDev& geo, const int16_t* first,
 void launch_compact(const Frame* frames, const int32_t* keep, const int64_t* offs, int64_t n,
                     Frame* out, int64_t* out_index, cudaStream_t st) {
   k_compact<<<grid_for(n), 256, 0, st>>>(frames, keep, offs, n, out, out_index);
+}
+
+namespace {
+__global__ void k_lor_keys(const Frame* __restrict__ frames, int32_t n, int32_t* keys,
+                           int32_t* index) {
+  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    keys[i] = frames[i].lor;
+    index[i] = i;
+  }
+}
+__global__ void k_gather_frames(const Frame* __restrict__ frames, const int32_t* index,
+                                int32_t n, Frame* out) {
+  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = frames[index[i]];
+}
+}  // namespace
+
+cudaError_t order_frames_by_lor(const Frame* frames, int32_t n, int64_t n_lors, Frame* out,
+                                cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  int end_bit = 1;
+  while (end_bit < 31 && ((int64_t)1 << end_bit) < n_lors) ++end_bit;
+  int32_t *keys = nullptr, *index = nullptr;
+  void* temp = nullptr;
+  size_t temp_bytes = 0;
+  cudaError_t e = cudaMalloc(&keys, 4 * (size_t)n * sizeof(int32_t));
+  if (e != cudaSuccess) return e;
+  index = keys + n;
+  int32_t* keys_out = keys + 2 * (size_t)n;
+  int32_t* index_out = keys + 3 * (size_t)n;
+  k_lor_keys<<<grid_for(n), 256, 0, st>>>(frames, n, keys, index);
+  e = cub::DeviceRadixSort::SortPairs(nullptr, temp_bytes, keys, keys_out, index, index_out, n,
+                                      0, end_bit, st);
+  if (e == cudaSuccess) e = cudaMalloc(&temp, temp_bytes);
+  if (e == cudaSuccess)
+    e = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys, keys_out, index, index_out, n,
+                                        0, end_bit, st);
+  if (e == cudaSuccess) {
+    k_gather_frames<<<grid_for(n), 256, 0, st>>>(frames, index_out, n, out);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(temp);
+  cudaFree(keys);
+  return e;
 }
 
 }  // namespace hybridmlem

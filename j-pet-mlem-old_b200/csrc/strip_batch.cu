@@ -45,6 +45,7 @@ struct strip_batch {
   BatchItem* d_items = nullptr;
   int n_items = 0;
   int cls_begin[2] = {0, 0}, cls_count[2] = {0, 0}, cls_smem[2] = {0, 0};
+  int cls_rows[2] = {0, 0};  // the most box rows of a class's events
   int* d_counter = nullptr;  // one counter per class
   int64_t n_events = 0;
   int launches_per_step = 0;
@@ -93,8 +94,8 @@ int enqueue_step(strip_batch* b) {
     if (b->cls_count[c] > 0)
       BCK(launch_tile_batch(b->mode, b->accum, *b->args,
                             b->d_items + b->cls_begin[c], b->cls_count[c],
-                            b->d_counter + c, b->cls_smem[c], b->sm_count,
-                            b->stream));
+                            b->d_counter + c, b->cls_smem[c], b->cls_rows[c],
+                            b->sm_count, b->stream));
   BatchUpdateArgs u{};
   u.n = (int)b->members.size();
   u.weighted = mlem_weighted(b->mode);
@@ -156,6 +157,7 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
     b->args->member[m] = ctx_mlem_args(c, mode);
     const int cls = c->t.smem_bytes > kNarrowSmem;
     b->cls_smem[cls] = std::max(b->cls_smem[cls], c->t.smem_bytes);
+    b->cls_rows[cls] = std::max(b->cls_rows[cls], c->t.max_rows);
     b->n_events += c->n_events;
     for (int i = 0; i < b->args->member[m].n_items; ++i) {
       const WorkItem& w = c->items[i];
@@ -202,7 +204,8 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
       bool attr_ok = true;
       for (int c = 0; c < 2; ++c)
         if (b->cls_count[c] > 0 &&
-            tile_batch_reserve_smem(b->mode, b->accum, b->cls_smem[c]) != cudaSuccess)
+            tile_batch_reserve_smem(b->mode, b->accum, b->cls_smem[c], b->cls_rows[c]) !=
+                cudaSuccess)
           attr_ok = false;
       if (!attr_ok ||
           cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {

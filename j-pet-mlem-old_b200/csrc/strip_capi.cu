@@ -223,7 +223,8 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
                       cudaMemcpyDeviceToHost, st));
   CKB(cudaStreamSynchronize(st));
 
-  const Tiling t = choose_tiling(ctx, wh[0], wh[1]);
+  Tiling t = choose_tiling(ctx, wh[0], wh[1]);
+  t.max_rows = wh[1];
   const int n_keys = n_subsets * (t.n_tiles + 1);
   CKB(cudaMalloc(&d_hist, (size_t)n_keys * sizeof(unsigned long long)));
   CKB(cudaMemsetAsync(d_hist, 0, (size_t)n_keys * sizeof(unsigned long long),

@@ -63,6 +63,7 @@ struct Tiling {
   int TX, TY, HX, HY, ntx, nty, n_tiles;
   int WXmax, WYmax, WS;
   int smem_bytes;  // the two shared-memory windows
+  int max_rows;    // the most box rows of any event (the kernels' lane layout)
 };
 
 __host__ __device__ inline void tile_window(const Tiling& t, int n_z, int n_y,
@@ -190,10 +191,11 @@ cudaError_t launch_gather_weights(const int64_t* perm, const double* w,
                                   int64_t n, float* out, cudaStream_t st);
 // Sets the batched tile kernel's dynamic shared-memory limit (before a
 // launch is captured into a graph).
-cudaError_t tile_batch_reserve_smem(int mode, int accum, int smem_bytes);
+// max_rows: the most box rows of any event of the launch's members.
+cudaError_t tile_batch_reserve_smem(int mode, int accum, int smem_bytes, int max_rows);
 cudaError_t launch_tile_batch(int mode, int accum, const BatchArgs& b,
                               const BatchItem* items, int n_items, int* counter,
-                              int smem_bytes, int sm_count, cudaStream_t st);
+                              int smem_bytes, int max_rows, int sm_count, cudaStream_t st);
 cudaError_t launch_update_batch(const BatchUpdateArgs& u, int64_t max_pix,
                                 cudaStream_t st);
 cudaError_t launch_sensitivity(const ScannerF& s, int five_point, float* out,

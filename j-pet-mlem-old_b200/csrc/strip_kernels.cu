@@ -35,6 +35,11 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
+// Threads of a tile CTA whose windows leave room for two CTAs per SM.
+#ifndef STRIP_TILE_THREADS
+#define STRIP_TILE_THREADS 512
+#endif
+constexpr int kTileThreads = STRIP_TILE_THREADS;
 // Tile kernels whose shared-memory windows leave room for one CTA per SM
 // run 1024-thread CTAs (32 warps, 64 registers each), so the SM keeps as
 // many resident warps as with two 512-thread CTAs.
@@ -47,19 +52,36 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-__device__ __forceinline__ EventF shfl_event(const EventF& m, int src) {
+// A set-up event as a warp holds it until its turn: tan, y, z, sec and the
+// clamped box (columns and rows lie in [0, 32767]) in two words.  The
+// ellipse's A, B, C follow from tan and sec (and the scanner) by the same
+// rounded binary32 operations as in event_setup, so they are formed again
+// when the event is taken (fewer registers held through the walks).
+struct EventPack {
+  float tan, y, z, sec;
+  unsigned x, yb;  // tlx | brx << 16, tly | bry << 16
+};
+__device__ __forceinline__ EventPack pack_event(const EventF& e) {
+  return EventPack{e.tan, e.y, e.z, e.sec, (unsigned)e.tlx | ((unsigned)e.brx << 16),
+                   (unsigned)e.tly | ((unsigned)e.bry << 16)};
+}
+__device__ __forceinline__ EventF shfl_event(const ScannerF& s, const EventPack& m, int src) {
   EventF e;
   e.tan = __shfl_sync(kFull, m.tan, src);
   e.y = __shfl_sync(kFull, m.y, src);
   e.z = __shfl_sync(kFull, m.z, src);
   e.sec = __shfl_sync(kFull, m.sec, src);
-  e.A = __shfl_sync(kFull, m.A, src);
-  e.B = __shfl_sync(kFull, m.B, src);
-  e.C = __shfl_sync(kFull, m.C, src);
-  e.tlx = __shfl_sync(kFull, m.tlx, src);
-  e.tly = __shfl_sync(kFull, m.tly, src);
-  e.brx = __shfl_sync(kFull, m.brx, src);
-  e.bry = __shfl_sync(kFull, m.bry, src);
+  const unsigned x = __shfl_sync(kFull, m.x, src), yb = __shfl_sync(kFull, m.yb, src);
+  e.tlx = (int)(x & 0xFFFFu);
+  e.brx = (int)(x >> 16);
+  e.tly = (int)(yb & 0xFFFFu);
+  e.bry = (int)(yb >> 16);
+  // gaussian_kernel.h:120-122, as event_setup
+  const float tt = __fmul_rn(e.tan, e.tan);
+  e.A = __fadd_rn(__fmul_rn(__fmul_rn(__fmul_rn(4.0f, e.sec), e.sec), s.ipsdl),
+                  __fmul_rn(__fmul_rn(2.0f, tt), s.ipsz));
+  e.B = __fmul_rn(__fmul_rn(-4.0f, e.tan), s.ipsz);
+  e.C = __fmul_rn(2.0f, s.ipsz);
   return e;
 }
 
@@ -254,61 +276,121 @@ __device__ __forceinline__ void walk_share(const RowTables& T, int nrows,
 }
 
 // ---------------------------------------------------------------------------
-// Lane-per-row event processing.  The box rows of an event are ranked
-// middle-out (the centre row first, then alternately below and above), so a
-// block of 32 consecutive ranks holds rows of similar run length; lane l of
-// block k owns the row of rank 32k + l.  A lane keeps its rows' run (lo, len)
-// and recurrence state (K0, R0) in registers across both passes: pass 1
-// walks its runs with K <- K*R, R <- R*q (no per-pixel exponential, no
-// per-pixel bookkeeping), pass 2 walks them again from the stored state.
-// Events with more than kRowBlocks*32 rows are processed in super-blocks and
-// rebuilt for pass 2.
+// Lane-per-row event processing.  An event is worked on by a group of LPE
+// lanes: a whole warp, or a half-warp (two events per warp).  The box rows
+// of an event are ranked middle-out (the centre row first, then alternately
+// below and above), so a block of LPE consecutive ranks holds rows of
+// similar run length; lane l of the group owns, in block k, the row of rank
+// LPE k + l.  A lane keeps its rows' run (lo, len) and recurrence state
+// (K0, R0) in registers across both passes: pass 1 walks its runs with
+// K <- K*R, R <- R*q (no per-pixel exponential, no per-pixel bookkeeping),
+// pass 2 walks them again from the stored state.  Events with more than
+// LPE * row_blocks rows are processed in super-blocks and rebuilt for pass 2.
+//
+// The GaussianKernel's MLEM, forward and adjoint give each event a half-warp:
+// 16-row blocks follow an ellipse's run lengths (longest in the middle rows,
+// shortest at the tips) more closely than 32-row blocks, so fewer lanes idle
+// in the set-up and in the walks (each block walks as long as its longest
+// run), and two events share the per-event shuffles and reductions.  The
+// AnalyticKernel (six row constants a block) and the sigma gradient keep one
+// event per warp.
 // ---------------------------------------------------------------------------
-constexpr int kRowBlocks = 3;
+#ifndef STRIP_LPE
+#define STRIP_LPE 16
+#endif
+template <int OP, int MODE>
+__host__ __device__ constexpr int lanes_per_event() {
+  return (MODE == STRIP_MODE_CPU && OP != OP_GRAD) ? STRIP_LPE : 32;
+}
+// Row blocks a lane keeps in registers (a super-block is LPE * blocks rows).
+// MLEM keeps its rows for both passes: with half-warps 5 blocks hold the at
+// most 76 box rows of sigma_dl = 25 mm on 1 mm pixels in one super-block.
+// The persistent batch kernel, whose members' constants take registers of
+// their own, keeps 4 (64 rows).  The forward and adjoint walk each row once,
+// so smaller super-blocks cost them only the loop, and free registers.
+#ifndef STRIP_MLEM_BLOCKS
+#define STRIP_MLEM_BLOCKS 5
+#endif
+#ifndef STRIP_BATCH_BLOCKS
+#define STRIP_BATCH_BLOCKS 4
+#endif
+#ifndef STRIP_PROJ_BLOCKS
+#define STRIP_PROJ_BLOCKS 3
+#endif
+template <int OP, int LPE, bool BATCH = false>
+__host__ __device__ constexpr int row_blocks() {
+  return LPE == 32        ? 3
+         : OP != OP_MLEM  ? STRIP_PROJ_BLOCKS
+         : BATCH          ? STRIP_BATCH_BLOCKS
+                          : STRIP_MLEM_BLOCKS;
+}
+// Whether a launch whose tallest event box has max_rows rows gives its events
+// half-warps (where lanes_per_event allows): MLEM only when one super-block
+// holds every event, since past it pass 2 rebuilds the rows of the further
+// super-blocks (a whole warp's 96-row super-block suits taller boxes, e.g.
+// the up to 126 rows of sigma_dl = 42 mm on 1 mm pixels, better: measured
+// on the 64-instance batch); the forward and adjoint walk each row once and
+// always do.
+#ifndef STRIP_BATCH_HALF
+#define STRIP_BATCH_HALF 1
+#endif
+__host__ __device__ constexpr bool half_warp_events(int op, int max_rows, bool batch = false) {
+  return batch ? STRIP_BATCH_HALF && max_rows <= 16 * STRIP_BATCH_BLOCKS
+               : op != OP_MLEM || max_rows <= 16 * STRIP_MLEM_BLOCKS;
+}
+
+// Sum over the lanes of one event's group (every lane of the warp calls it).
+template <int LPE>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = LPE / 2; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
 // Walk GaussianKernel runs two pixels per step with packed f32x2 arithmetic.
 #ifndef STRIP_PAIRS
 #define STRIP_PAIRS 1
 #endif
 constexpr bool kPairs = STRIP_PAIRS != 0;
 
-template <int MODE>
+template <int MODE, int NB>
 struct LaneRows;
 
 // Run of block b: run[b] = the window's packed run (len == 0: no run).
 __device__ __forceinline__ int run_len(unsigned v) { return (int)(v & 0xFFFFu); }
 
 // GaussianKernel: K along the run from K0 = K(t0) and the ratio R0
-template <>
-struct LaneRows<STRIP_MODE_CPU> {
-  unsigned run[kRowBlocks];
-  float K0[kRowBlocks], R0[kRowBlocks];
+template <int NB>
+struct LaneRows<STRIP_MODE_CPU, NB> {
+  unsigned run[NB];
+  float K0[NB], R0[NB];
 };
 // AnalyticKernel: direct evaluation per pixel from the row constants
-template <>
-struct LaneRows<STRIP_MODE_GPU> {
-  unsigned run[kRowBlocks];
-  float t0[kRowBlocks], n0[kRowBlocks], n1[kRowBlocks], u0[kRowBlocks],
-      u1[kRowBlocks], cr[kRowBlocks];
+template <int NB>
+struct LaneRows<STRIP_MODE_GPU, NB> {
+  unsigned run[NB];
+  float t0[NB], n0[NB], n1[NB], u0[NB], u1[NB], cr[NB];
 };
 
-// Builds the lane's rows of ranks [rank0, rank0 + 32*kRowBlocks).
-template <int MODE, bool CLOSED_ONLY, class Win>
+// Builds the lane's rows of ranks rank0 + LPE * b + sub (b < NB) of an event
+// of H rows (H = 0: no rows).
+template <int MODE, bool CLOSED_ONLY, int LPE, int NB, class Win>
 __device__ __forceinline__ void build_lane_rows_t(const ScannerF& s,
                                                 const KernelF& k,
                                                 const EventF& e,
                                                 const EventRows& er,
                                                 const GaussEvent& ge, int H,
-                                                int rank0, int lane,
+                                                int rank0, int sub,
                                                 const Win& win,
-                                                LaneRows<MODE>& L) {
+                                                LaneRows<MODE, NB>& L) {
 #pragma unroll
-  for (int b = 0; b < kRowBlocks; ++b) {
+  for (int b = 0; b < NB; ++b) {
     L.run[b] = 0u;
     if constexpr (MODE == STRIP_MODE_CPU) {  // rows without a run walk nothing
       L.K0[b] = 0.0f;
       L.R0[b] = 0.0f;
     }
-    const int i = rank0 + 32 * b + lane;
+    const int i = rank0 + LPE * b + sub;
     if (i < H) {
       const int iy = e.tly + ranked_row(H, i);
       const RowSet rs = row_set(s, e, iy);
@@ -336,35 +418,36 @@ __device__ __forceinline__ void build_lane_rows_t(const ScannerF& s,
 
 // The same, with the row runs' general search compiled out when the
 // geometry lets the closed form settle every row (uniform per launch).
-template <int MODE, class Win>
+template <int MODE, int LPE, int NB, class Win>
 __device__ __forceinline__ void build_lane_rows(const ScannerF& s,
                                                 const KernelF& k,
                                                 const EventF& e,
                                                 const EventRows& er,
                                                 const GaussEvent& ge, int H,
-                                                int rank0, int lane,
+                                                int rank0, int sub,
                                                 const Win& win,
-                                                LaneRows<MODE>& L) {
+                                                LaneRows<MODE, NB>& L) {
   if (s.min_closed_hw == 0.0f)
-    build_lane_rows_t<MODE, true>(s, k, e, er, ge, H, rank0, lane, win, L);
+    build_lane_rows_t<MODE, true, LPE>(s, k, e, er, ge, H, rank0, sub, win, L);
   else
-    build_lane_rows_t<MODE, false>(s, k, e, er, ge, H, rank0, lane, win, L);
+    build_lane_rows_t<MODE, false, LPE>(s, k, e, er, ge, H, rank0, sub, win, L);
 }
 
-// Pass 1 over the lane's rows: sum over runs of K_j * w_j.
-template <int MODE, int ACC, class Win>
+// Pass 1 over the lane's rows: sum over runs of K_j * w_j.  nb (the blocks
+// to walk) is the same in every lane of the warp.
+template <int MODE, int ACC, int LPE, int NB, class Win>
 __device__ __forceinline__ void pass1_rows(const ScannerF& s, const KernelF& k,
                                            const EventF& e, int H, int rank0,
-                                           int lane, const LaneRows<MODE>& L,
+                                           int sub, const LaneRows<MODE, NB>& L,
                                            int nb, const Win& win,
                                            RowSum<ACC>& acc) {
 #pragma unroll
-  for (int b = 0; b < kRowBlocks; ++b) {
+  for (int b = 0; b < NB; ++b) {
     const int n = run_len(L.run[b]);
     // every lane enters (a lane without a run walks n = 0 pixels): the warp
     // stays converged instead of branching around empty rows
     if (b < nb) {
-      const auto p = win.run_ptr(L.run[b], e, H, rank0 + 32 * b + lane);
+      const auto p = win.run_ptr(L.run[b], e, H, rank0 + LPE * b + sub);
       float a = 0.0f;
       if constexpr (MODE == STRIP_MODE_CPU && kPairs && Win::kShared) {
         // two pixels per step: a count-down loop over pairs, one shared
@@ -419,24 +502,25 @@ __device__ __forceinline__ void pass1_rows(const ScannerF& s, const KernelF& k,
 }
 
 // Pass 2 over the lane's rows: acc_j += K_j * scale, or, WEIGHTED (MLEM with
-// the reference CPU semantics), acc_j += K_j * w_j * scale.
-template <int MODE, bool WEIGHTED, class Win>
+// the reference CPU semantics), acc_j += K_j * w_j * scale.  A lane whose
+// event does not scatter (go false) walks no pixels.
+template <int MODE, bool WEIGHTED, int LPE, int NB, class Win>
 __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
                                            const EventF& e, int H, int rank0,
-                                           int lane, const LaneRows<MODE>& L,
+                                           int sub, const LaneRows<MODE, NB>& L,
                                            int nb, const Win& win,
-                                           float scale) {
+                                           float scale, bool go) {
   // the event's factor in the window's units (clamped: a denominator so
   // small that 1 / D overflows still scatters finite values)
   const float sc = WEIGHTED ? fminf(scale * win.unit(), 3.0e38f)
                             : scale * win.unit();
 #pragma unroll
-  for (int b = 0; b < kRowBlocks; ++b) {
-    const int n = run_len(L.run[b]);
+  for (int b = 0; b < NB; ++b) {
+    const int n = go ? run_len(L.run[b]) : 0;
     // every lane enters (a lane without a run walks n = 0 pixels): the warp
     // stays converged instead of branching around empty rows
     if (b < nb) {
-      const auto p = win.run_ptr(L.run[b], e, H, rank0 + 32 * b + lane);
+      const auto p = win.run_ptr(L.run[b], e, H, rank0 + LPE * b + sub);
       if constexpr (MODE == STRIP_MODE_CPU && WEIGHTED && Win::unweighted()) {
         // K / D in fixed point: no image reads, one conversion per pixel
         const float K0 = L.K0[b] * sc, R0 = L.R0[b], R2 = R0 * R0;
@@ -607,16 +691,37 @@ __device__ __forceinline__ void grad_event(const LaunchArgs& a,
   }
 }
 
-// One event on one warp.  Returns 1 / D_e for an MLEM event with a positive
-// denominator (the work item's statistic), 0 otherwise; -1 / D_e for an
-// event the unweighted window had no room for (not scattered: the caller
-// runs it again in a weighted window).
-template <int OP, int MODE, int ACC, class Win>
+// The event of lane src of the warp's set-up lanes (`mine`), or, when `has`
+// is false, an event without box rows.
+__device__ __forceinline__ EventF fetch_event(const ScannerF& s, const EventPack& mine,
+                                              int src, bool has) {
+  EventF e = shfl_event(s, mine, src);
+  if (!has) e.bry = e.tly;
+  return e;
+}
+
+// One event on a group of LPE lanes (every lane of the warp calls this; with
+// LPE = 16 the two half-warps bring two events, and an empty event has no
+// box rows): the event of set-up lane src (has: there is one).  Returns, in
+// the event's lanes, 1 / D_e for an MLEM event with a positive denominator
+// (the work item's statistic), 0 otherwise; -1 / D_e for an event the
+// unweighted window had no room for (not scattered: the caller runs it again
+// in a weighted window).  The event's set-up values are not kept through
+// pass 2: the rare events whose rows need a second super-block fetch the
+// event again (fewer live registers in the walks).
+template <int OP, int MODE, int ACC, int LPE, int NB, class Win>
 __device__ __forceinline__ float process_event(const LaunchArgs& a,
-                                               const EventF& e, const Win& win,
+                                               const EventPack& mine, int src, bool has,
+                                               const Win& win,
                                                int lane, const EventAux& aux) {
-  const int H = e.bry - e.tly;
-  if (H <= 0 || e.brx <= e.tlx) return 0.0f;
+  static_assert(LPE == 32 || LPE == 16, "a warp or a half-warp per event");
+  static_assert(OP != OP_GRAD || LPE == 32, "the sigma gradient takes a warp");
+  const EventF e = fetch_event(a.s, mine, src, has);
+  const int sub = lane & (LPE - 1);
+  const int H = (e.bry > e.tly && e.brx > e.tlx) ? e.bry - e.tly : 0;
+  int Hw = H;  // the warp's largest, for loop bounds the whole warp shares
+  if constexpr (LPE < 32) Hw = max(Hw, __shfl_xor_sync(kFull, Hw, 16));
+  if (Hw == 0) return 0.0f;
   const EventRows er = event_rows(a.s, e);
   if constexpr (OP == OP_GRAD) {
     grad_event(a, e, er, H, win, lane, aux.w);
@@ -624,56 +729,67 @@ __device__ __forceinline__ float process_event(const LaunchArgs& a,
   }
   GaussEvent ge{};
   if constexpr (MODE == STRIP_MODE_CPU) ge.init(a.k, a.s.R, e.tan, e.sec);
-  constexpr int kSuper = 32 * kRowBlocks;
-  LaneRows<MODE> L;
+  constexpr int kSuper = LPE * NB;
+  LaneRows<MODE, NB> L;
   float scale;
+  bool go;  // this lane's event scatters
   if (OP == OP_MLEM || OP == OP_FORWARD) {
     RowSum<ACC> acc;
     // super-blocks of rows last to first, so that the registers end holding
     // the first (the middle rows, the longest runs): pass 2 rebuilds only
     // the others
-    for (int r0 = ((H - 1) / kSuper) * kSuper; r0 >= 0; r0 -= kSuper) {
-      build_lane_rows<MODE>(a.s, a.k, e, er, ge, H, r0, lane, win, L);
-      pass1_rows<MODE, ACC>(a.s, a.k, e, H, r0, lane, L,
-                            min(kRowBlocks, (H - r0 + 31) >> 5), win, acc);
+    for (int r0 = ((Hw - 1) / kSuper) * kSuper; r0 >= 0; r0 -= kSuper) {
+      build_lane_rows<MODE, LPE>(a.s, a.k, e, er, ge, H, r0, sub, win, L);
+      pass1_rows<MODE, ACC, LPE>(a.s, a.k, e, H, r0, sub, L,
+                                 min(NB, (Hw - r0 + LPE - 1) / LPE), win, acc);
     }
-    const double D = warp_sum(acc.total());
+    const double D = group_sum<LPE>(acc.total());
     if (OP == OP_FORWARD) {
-      if (lane == 0) a.y_out[aux.out] = D;
+      if (sub == 0 && H > 0) a.y_out[aux.out] = D;
       return 0.0f;
     }
     // reconstruction.h:290 -- an all-zero denominator contributes nothing
-    if (!(D > 0.0)) return 0.0f;
-    scale = rcp_approx((float)D);  // within an ulp of 1 / D; 0 or inf at the range ends
+    go = H > 0 && D > 0.0;
+    scale = go ? rcp_approx((float)D) : 0.0f;  // within an ulp of 1 / D; 0 or inf at the range ends
   } else {
     scale = aux.wf;  // OP_ADJOINT
-    if (scale == 0.0f) return 0.0f;
+    go = H > 0 && scale != 0.0f;
   }
+  float ret = go ? scale : 0.0f;
   if constexpr (Win::unweighted()) {
     // reserve the event's largest addend, kbound * unit / D (rounded up, in
     // units of 2^8), from the item's fixed-point budget
     const float need = a.kbound * scale * win.unit();
     int ok = 0;
-    if (lane == 0 && need < kFixedBudget) {
+    if (sub == 0 && go && need < kFixedBudget) {
       const unsigned nu = (unsigned)(need * (1.0f / 256.0f)) + 1u;
       const unsigned old = atomicAdd(&s_fx_budget, nu);
       ok = old + nu <= kBudgetUnits;
       if (!ok) atomicSub(&s_fx_budget, nu);
     }
-    if (!__shfl_sync(kFull, ok, 0)) return -scale;
+    ok = __shfl_sync(kFull, ok, lane & ~(LPE - 1));
+    if (go && !ok) {
+      ret = -scale;
+      go = false;
+    }
   }
+  if (!__any_sync(kFull, go)) return OP == OP_MLEM ? ret : 0.0f;
   constexpr bool kWeighted = OP == OP_MLEM && MODE == STRIP_MODE_CPU;
   if (OP == OP_MLEM) {  // the registers hold the first super-block
-    pass2_rows<MODE, kWeighted>(a.s, a.k, e, H, 0, lane, L,
-                                min(kRowBlocks, (H + 31) >> 5), win, scale);
-    if (H <= kSuper) return scale;
+    pass2_rows<MODE, kWeighted, LPE>(a.s, a.k, e, H, 0, sub, L,
+                                     min(NB, (Hw + LPE - 1) / LPE), win, scale, go);
+    if (Hw <= kSuper) return ret;
   }
-  for (int r0 = OP == OP_MLEM ? kSuper : 0; r0 < H; r0 += kSuper) {
-    build_lane_rows<MODE>(a.s, a.k, e, er, ge, H, r0, lane, win, L);
-    pass2_rows<MODE, kWeighted>(a.s, a.k, e, H, r0, lane, L,
-                                min(kRowBlocks, (H - r0 + 31) >> 5), win, scale);
+  const EventF e2 = OP == OP_MLEM ? fetch_event(a.s, mine, src, has) : e;
+  const EventRows er2 = OP == OP_MLEM ? event_rows(a.s, e2) : er;
+  GaussEvent ge2 = ge;
+  if constexpr (OP == OP_MLEM && MODE == STRIP_MODE_CPU) ge2.init(a.k, a.s.R, e2.tan, e2.sec);
+  for (int r0 = OP == OP_MLEM ? kSuper : 0; r0 < Hw; r0 += kSuper) {
+    build_lane_rows<MODE, LPE>(a.s, a.k, e2, er2, ge2, H, r0, sub, win, L);
+    pass2_rows<MODE, kWeighted, LPE>(a.s, a.k, e2, H, r0, sub, L,
+                                     min(NB, (Hw - r0 + LPE - 1) / LPE), win, scale, go);
   }
-  return OP == OP_MLEM ? scale : 0.0f;
+  return OP == OP_MLEM ? ret : 0.0f;
 }
 
 __device__ __forceinline__ RowTables warp_tables(char* base, int cap, int warp) {
@@ -715,14 +831,16 @@ __device__ int adjoint_shift(const LaunchArgs& a, const WorkItem& it, int lane) 
 // events up in parallel).  With `only`, just the events whose bit is set:
 // the rerun, in a weighted window, of the events an unweighted window had no
 // room for (their 1 / D_e is counted already).
-template <int OP, int MODE, int ACC, class Win>
+template <int OP, int MODE, int ACC, int LPE, int NB, class Win>
 __device__ __forceinline__ void run_item(const LaunchArgs& a, const WorkItem& it,
                                          const Win& win, int lane,
                                          int* next_group,
                                          const unsigned* only = nullptr) {
+  constexpr int kPerWarp = 32 / LPE;  // events the warp works on at once
+  const int half = lane / LPE;        // this lane's event of the kPerWarp
   const int64_t end = it.begin + it.count;
   const int grab = a.grab;
-  float rsum = 0.0f;  // this warp's sum of 1 / D_e
+  float rsum = 0.0f;  // the sum of 1 / D_e of this lane's events
   for (;;) {
     int g = 0;
     if (lane == 0) g = atomicAdd(next_group, 1);
@@ -730,21 +848,25 @@ __device__ __forceinline__ void run_item(const LaunchArgs& a, const WorkItem& it
     const int64_t base = it.begin + (int64_t)g * grab;
     if (base >= end) break;
     const int64_t ei = base + lane;
-    EventF mine = {};
+    EventPack mine = {};
     EventAux aux;
     if (lane < grab && ei < end) {
       const int off = (int)(ei - it.begin);
       if (!only || ((only[off >> 5] >> (off & 31)) & 1u)) {
         aux = load_aux<OP>(a, ei);
-        event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], mine);
+        EventF ev;
+        event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], ev);
+        mine = pack_event(ev);
       }
     }
     const int nh = (int)min((int64_t)grab, end - base);
-    for (int j = 0; j < nh; ++j) {
-      const EventF e = shfl_event(mine, j);
-      const float r = process_event<OP, MODE, ACC>(a, e, win, lane, shfl_aux<OP>(aux, j));
+    for (int j0 = 0; j0 < nh; j0 += kPerWarp) {
+      const int j = j0 + half;
+      const bool has = j < nh;  // no event for this half: no rows
+      const float r = process_event<OP, MODE, ACC, LPE, NB>(
+          a, mine, has ? j : j0, has, win, lane, shfl_aux<OP>(aux, has ? j : j0));
       if (r < 0.0f) {  // not scattered: no room in the unweighted window
-        if (lane == 0) {
+        if ((lane & (LPE - 1)) == 0) {
           const int off = (int)(base + j - it.begin);
           atomicOr(&s_fb_bits[off >> 5], 1u << (off & 31));
           atomicAdd(&s_fb_n, 1);
@@ -755,7 +877,8 @@ __device__ __forceinline__ void run_item(const LaunchArgs& a, const WorkItem& it
       }
     }
   }
-  if (OP == OP_MLEM && lane == 0 && !only && rsum != 0.0f) atomicAdd(&s_item_rsum, rsum);
+  if (OP == OP_MLEM && (lane & (LPE - 1)) == 0 && !only && rsum != 0.0f)
+    atomicAdd(&s_item_rsum, rsum);
 }
 
 // Sum of v over the CTA, returned to every thread (two barriers).
@@ -779,7 +902,7 @@ __device__ __forceinline__ float block_sum(float v) {
 // `index` is the item's index among the launch's items (its statistic in
 // a.item_hist).  The CTA may run further items afterwards (the batched
 // kernel): the caller synchronises before the shared memory is reused.
-template <int OP, int MODE, int ACC>
+template <int OP, int MODE, int ACC, int LPE, int NB>
 __device__ __forceinline__ void tile_item(const LaunchArgs& a,
                                           const WorkItem it, int index,
                                           char* smem_raw, int* s_next_group) {
@@ -844,7 +967,7 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
   // or all); returns its scale's exponent.
   auto run_weighted = [&](int count, const unsigned* only) {
     const int fs = fixed_shift(count);
-    run_item<OP, MODE, ACC>(
+    run_item<OP, MODE, ACC, LPE, NB>(
         a, it, SmemWin<kAccU32Cvt>{s_w, s_acc, wx0, wy0, WS, exp2f((float)fs), w_sh, acc_sh},
         lane, s_next_group, only);
     return fs;
@@ -863,7 +986,7 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
       unweighted = fshift >= -120 && fshift <= 120;
     }
     if (unweighted) {
-      run_item<OP, MODE, ACC>(
+      run_item<OP, MODE, ACC, LPE, NB>(
           a, it,
           SmemWin<kAccU32Unw>{s_w, s_acc, wx0, wy0, WS, exp2f((float)fshift), w_sh, acc_sh},
           lane, s_next_group);
@@ -889,14 +1012,14 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
     if (threadIdx.x == 0 && a.item_hist) a.item_hist[index] = s_item_rsum * wmean;
   } else if constexpr (OP == OP_ADJOINT && MODE == STRIP_MODE_CPU) {
     const int fshift = adjoint_shift(a, it, lane);
-    run_item<OP, MODE, ACC>(
+    run_item<OP, MODE, ACC, LPE, NB>(
         a, it,
         SmemWin<kAccS32>{s_w, s_acc, wx0, wy0, WS, exp2f((float)fshift), w_sh, acc_sh},
         lane, s_next_group);
     __syncthreads();
     flush(fshift, false);
   } else {
-    run_item<OP, MODE, ACC>(a, it,
+    run_item<OP, MODE, ACC, LPE, NB>(a, it,
                             SmemWin<kAccF32>{s_w, s_acc, wx0, wy0, WS, 1.0f, w_sh, acc_sh},
                             lane, s_next_group);
     if (kWrites) {
@@ -910,34 +1033,37 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
 // and accumulator) and up to 64 registers a thread (2 x 16 warps per SM);
 // the GaussianKernel forward and adjoint keep one window each and fit 40
 // registers, for 3 x 16 warps.
+#ifndef STRIP_FWD_CTAS
+#define STRIP_FWD_CTAS 3
+#endif
 #ifndef STRIP_ADJ_CTAS
 #define STRIP_ADJ_CTAS 3
 #endif
 template <int OP, int MODE>
 constexpr int tile_ctas_per_sm() {
   return MODE != STRIP_MODE_CPU ? 2
-         : OP == OP_FORWARD    ? 3
+         : OP == OP_FORWARD    ? STRIP_FWD_CTAS
          : OP == OP_ADJOINT    ? STRIP_ADJ_CTAS
                                : 2;
 }
 template <int OP>
 constexpr int tile_windows() { return OP == OP_MLEM ? 2 : 1; }
 
-template <int OP, int MODE, int ACC, int THREADS>
+template <int OP, int MODE, int ACC, int THREADS, int LPE>
 __global__ void __launch_bounds__(THREADS, THREADS == kWideThreads
                                                ? 1
                                                : tile_ctas_per_sm<OP, MODE>())
     k_tile(const __grid_constant__ LaunchArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   __shared__ int s_next_group;
-  tile_item<OP, MODE, ACC>(a, a.items[blockIdx.x], blockIdx.x, smem_raw,
-                           &s_next_group);
+  tile_item<OP, MODE, ACC, LPE, row_blocks<OP, LPE>()>(a, a.items[blockIdx.x], blockIdx.x,
+                                                       smem_raw, &s_next_group);
 }
 
 // Persistent tile kernel over the work items of several reconstructions: a
 // CTA takes item after item from a global counter; item i belongs to member
 // items[i].member, whose arguments live in the kernel's parameter space.
-template <int MODE, int ACC, int THREADS>
+template <int MODE, int ACC, int THREADS, int LPE>
 __global__ void __launch_bounds__(THREADS, THREADS == kWideThreads ? 1 : 2)
     k_tile_batch(const __grid_constant__ BatchArgs b, const BatchItem* items,
                  int n_items, int* counter) {
@@ -950,7 +1076,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == kWideThreads ? 1 : 2)
     const int i = s_item;
     if (i >= n_items) break;
     const BatchItem bi = items[i];
-    tile_item<OP_MLEM, MODE, ACC>(b.member[bi.member],
+    tile_item<OP_MLEM, MODE, ACC, LPE, row_blocks<OP_MLEM, LPE, true>()>(b.member[bi.member],
                                   WorkItem{bi.tile, bi.count, bi.begin},
                                   bi.index, smem_raw, &s_next_group);
     __syncthreads();  // before the next item's window overwrites this one
@@ -976,23 +1102,30 @@ __global__ void k_update_batch(const __grid_constant__ BatchUpdateArgs u) {
 
 template <int OP, int MODE, int ACC>
 __global__ void __launch_bounds__(kThreads) k_global(LaunchArgs a) {
+  constexpr int LPE = lanes_per_event<OP, MODE>();
+  constexpr int kPerWarp = 32 / LPE;
   const GlobalWin<MODE> win{a.rho, a.sens, a.acc, a.s.n_z};
   const int lane = threadIdx.x & 31;
+  const int half = lane / LPE;
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwt = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t end = a.g_begin + a.g_count;
   for (int64_t base = a.g_begin + wid * 32; base < end; base += nwt * 32) {
     const int64_t ei = base + lane;
-    EventF mine = {};
+    EventPack mine = {};
     EventAux aux;
     if (ei < end) {
       aux = load_aux<OP>(a, ei);
-      event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], mine);
+      EventF ev;
+      event_setup(a.s, a.zu[ei], a.zd[ei], a.dl[ei], ev);
+      mine = pack_event(ev);
     }
     const int nh = (int)min((int64_t)32, end - base);
-    for (int j = 0; j < nh; ++j) {
-      const EventF e = shfl_event(mine, j);
-      process_event<OP, MODE, ACC>(a, e, win, lane, shfl_aux<OP>(aux, j));
+    for (int j0 = 0; j0 < nh; j0 += kPerWarp) {
+      const int j = j0 + half;
+      const bool has = j < nh;
+      process_event<OP, MODE, ACC, LPE, row_blocks<OP, LPE>()>(
+          a, mine, has ? j : j0, has, win, lane, shfl_aux<OP>(aux, has ? j : j0));
     }
   }
 }
@@ -1299,16 +1432,25 @@ int grid_for(int64_t n, int per_block = kThreads, int cap = 148 * 16) {
 
 constexpr int kSetsCap = 64;
 
-template <int OP, int MODE, int ACC>
-cudaError_t launch_tile_t(const LaunchArgs& a, cudaStream_t st) {
+template <int OP, int MODE, int ACC, int LPE>
+cudaError_t launch_tile_lpe(const LaunchArgs& a, cudaStream_t st) {
   const int smem = a.t.smem_bytes / 2 * tile_windows<OP>();
   const bool wide = smem > kNarrowSmemBytes;  // one CTA per SM: 1024 threads
-  auto fn = wide ? k_tile<OP, MODE, ACC, kWideThreads> : k_tile<OP, MODE, ACC, kThreads>;
+  auto fn = wide ? k_tile<OP, MODE, ACC, kWideThreads, LPE>
+                 : k_tile<OP, MODE, ACC, kTileThreads, LPE>;
   cudaError_t err = cudaFuncSetAttribute(
       fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (err != cudaSuccess) return err;
-  fn<<<a.n_items, wide ? kWideThreads : kThreads, smem, st>>>(a);
+  fn<<<a.n_items, wide ? kWideThreads : kTileThreads, smem, st>>>(a);
   return cudaGetLastError();
+}
+
+template <int OP, int MODE, int ACC>
+cudaError_t launch_tile_t(const LaunchArgs& a, cudaStream_t st) {
+  if constexpr (lanes_per_event<OP, MODE>() == 16) {
+    if (half_warp_events(OP, a.t.max_rows)) return launch_tile_lpe<OP, MODE, ACC, 16>(a, st);
+  }
+  return launch_tile_lpe<OP, MODE, ACC, 32>(a, st);
 }
 
 template <int OP, int MODE, int ACC>
@@ -1376,32 +1518,42 @@ cudaError_t launch_global(int op, int mode, int accum, const LaunchArgs& a,
 }
 
 template <int THREADS, class F>
-cudaError_t with_tile_batch_t(int mode, int accum, F&& pick) {
+cudaError_t with_tile_batch_t(int mode, int accum, bool half, F&& pick) {
   if (mode == STRIP_MODE_CPU) {
+    constexpr int H = lanes_per_event<OP_MLEM, STRIP_MODE_CPU>();
+    if (half) {
+      if (accum == STRIP_ACCUM_FP32)
+        return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP32, THREADS, H>);
+      if (accum == STRIP_ACCUM_FP64)
+        return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP64, THREADS, H>);
+      return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_KAHAN, THREADS, H>);
+    }
     if (accum == STRIP_ACCUM_FP32)
-      return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP32, THREADS>);
+      return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP32, THREADS, 32>);
     if (accum == STRIP_ACCUM_FP64)
-      return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP64, THREADS>);
-    return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_KAHAN, THREADS>);
+      return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP64, THREADS, 32>);
+    return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_KAHAN, THREADS, 32>);
   }
   if (accum == STRIP_ACCUM_FP32)
-    return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_FP32, THREADS>);
+    return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_FP32, THREADS, 32>);
   if (accum == STRIP_ACCUM_FP64)
-    return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_FP64, THREADS>);
-  return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_KAHAN, THREADS>);
+    return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_FP64, THREADS, 32>);
+  return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_KAHAN, THREADS, 32>);
 }
 
 // The persistent batch kernel of a shared-memory class: windows that fit two
-// CTAs per SM run 512-thread CTAs, wider ones 1024-thread CTAs, one per SM.
+// CTAs per SM run 512-thread CTAs, wider ones 1024-thread CTAs, one per SM;
+// half-warp events where every member's tallest box allows them.
 template <class F>
-cudaError_t with_tile_batch(int mode, int accum, int smem_bytes, F&& pick) {
+cudaError_t with_tile_batch(int mode, int accum, int smem_bytes, int max_rows, F&& pick) {
+  const bool half = half_warp_events(OP_MLEM, max_rows, true);
   if (smem_bytes > kNarrowSmemBytes)
-    return with_tile_batch_t<kWideThreads>(mode, accum, pick);
-  return with_tile_batch_t<kThreads>(mode, accum, pick);
+    return with_tile_batch_t<kWideThreads>(mode, accum, half, pick);
+  return with_tile_batch_t<kTileThreads>(mode, accum, half, pick);
 }
 
-cudaError_t tile_batch_reserve_smem(int mode, int accum, int smem_bytes) {
-  return with_tile_batch(mode, accum, smem_bytes, [&](auto fn) {
+cudaError_t tile_batch_reserve_smem(int mode, int accum, int smem_bytes, int max_rows) {
+  return with_tile_batch(mode, accum, smem_bytes, max_rows, [&](auto fn) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 smem_bytes);
   });
@@ -1409,15 +1561,15 @@ cudaError_t tile_batch_reserve_smem(int mode, int accum, int smem_bytes) {
 
 cudaError_t launch_tile_batch(int mode, int accum, const BatchArgs& b,
                               const BatchItem* items, int n_items, int* counter,
-                              int smem_bytes, int sm_count, cudaStream_t st) {
+                              int smem_bytes, int max_rows, int sm_count, cudaStream_t st) {
   if (n_items <= 0) return cudaSuccess;
   const bool wide = smem_bytes > kNarrowSmemBytes;
   auto pick = [&](auto fn) -> cudaError_t {
     const int grid = std::min(n_items, sm_count * (wide ? 1 : 2));
-    fn<<<grid, wide ? kWideThreads : kThreads, smem_bytes, st>>>(b, items, n_items, counter);
+    fn<<<grid, wide ? kWideThreads : kTileThreads, smem_bytes, st>>>(b, items, n_items, counter);
     return cudaGetLastError();
   };
-  return with_tile_batch(mode, accum, smem_bytes, pick);
+  return with_tile_batch(mode, accum, smem_bytes, max_rows, pick);
 }
 
 
