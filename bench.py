@@ -582,6 +582,9 @@ def ours(args, rank, world, local_rank):
         # host wall time of each phase (every call returns once its work is
         # done), summed over the timed steps
         phases = {"set_events": 0.0, "set_image": 0.0, "iterations": 0.0, "get_image": 0.0}
+        # within set_events: the host -> device copy (wall) and the binning
+        # (device time), from the context's statistics
+        sub = {"set_events_upload": 0.0, "set_events_binning": 0.0}
         with ClockSampler(local_rank) as clk_e2e:
             for s in range(args.e2e_steps + 1):
                 if dist is not None:
@@ -604,6 +607,9 @@ def ours(args, rank, world, local_rank):
                     times.append(a.elapsed_time(b) / 1e3)
                     for k, dt in zip(phases, (w1 - w0, w2 - w1, w3 - w2, w4 - w3)):
                         phases[k] += dt
+                    st_e = rec.stats()
+                    sub["set_events_upload"] += st_e["last_upload_ms"] / 1e3
+                    sub["set_events_binning"] += st_e["last_setup_ms"] / 1e3
         e2e_t = sum(times) / len(times)
         if dist is not None:
             tt = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
@@ -613,7 +619,8 @@ def ours(args, rank, world, local_rank):
                "unit": UNIT, "h2d_bytes_per_step": int(3 * 4 * n),
                "d2h_bytes_per_step": int(img.nbytes), "steps": len(times),
                "iterations_per_step": args.e2e_iters,
-               "phases_s_per_step": {k: v / len(times) for k, v in phases.items()},
+               "phases_s_per_step": {k: v / len(times)
+                                     for k, v in list(phases.items()) + list(sub.items())},
                "clocks": clk_e2e.summary(),
                "timed": "set_events (pinned host -> HBM, binning) + iterations + image D2H, "
                         "CUDA events, max over ranks"}

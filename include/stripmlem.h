@@ -105,6 +105,10 @@ typedef struct strip_stats {
                                 no room for (rerun in a weighted window)       */
   int32_t max_item_events;   /* events of the largest tile work item           */
   int32_t reserved;
+  double last_upload_ms;     /* host wall time of the last set_events /
+                                set_responses / load_responses_file copy of
+                                the events into device memory (file reads
+                                included), before the binning               */
 } strip_stats;
 
 /* ---- context ------------------------------------------------------------ */

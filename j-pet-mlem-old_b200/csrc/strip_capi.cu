@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -593,10 +594,13 @@ int strip_set_events(strip_ctx* ctx, const float* zu, const float* zd,
   float* dzd = d + std::max<int64_t>(n, 1);
   float* ddl = d + 2 * std::max<int64_t>(n, 1);
   if (n > 0) {
+    const auto t0 = std::chrono::steady_clock::now();
     if (int rc = upload_soa(ctx, zu, zd, dl, n, dzu, dzd, ddl)) {
       cudaFree(d);
       return rc;
     }
+    ctx->stats.last_upload_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
   ctx->n_events = n;
   int rc = bin_events(ctx, dzu, dzd, ddl, nullptr, n, n_subsets);

@@ -277,7 +277,7 @@ __device__ __forceinline__ void walk_share(const RowTables& T, int nrows,
 
 // ---------------------------------------------------------------------------
 // Lane-per-row event processing.  An event is worked on by a group of LPE
-// lanes: a whole warp, or a half-warp (two events per warp).  The box rows
+// lanes: a whole warp, a half-warp or a quarter-warp.  The box rows
 // of an event are ranked middle-out (the centre row first, then alternately
 // below and above), so a block of LPE consecutive ranks holds rows of
 // similar run length; lane l of the group owns, in block k, the row of rank
@@ -287,20 +287,27 @@ __device__ __forceinline__ void walk_share(const RowTables& T, int nrows,
 // pass 2 walks them again from the stored state.  Events with more than
 // LPE * row_blocks rows are processed in super-blocks and rebuilt for pass 2.
 //
-// The GaussianKernel's MLEM, forward and adjoint give each event a half-warp:
-// 16-row blocks follow an ellipse's run lengths (longest in the middle rows,
-// shortest at the tips) more closely than 32-row blocks, so fewer lanes idle
-// in the set-up and in the walks (each block walks as long as its longest
-// run), and two events share the per-event shuffles and reductions.  The
-// AnalyticKernel (six row constants a block) and the sigma gradient keep one
-// event per warp.
+// The GaussianKernel's MLEM gives each event a half-warp: 16-row blocks
+// follow an ellipse's run lengths (longest in the middle rows, shortest at
+// the tips) more closely than 32-row blocks, so fewer lanes idle in the
+// set-up and in the walks (each block walks as long as its longest run), and
+// two events share the per-event shuffles and reductions.  The forward and
+// adjoint, which keep no rows between passes, go further: a quarter-warp per
+// event, 8-row blocks, four events per warp.  The AnalyticKernel (six row
+// constants a block) and the sigma gradient keep one event per warp.
 // ---------------------------------------------------------------------------
 #ifndef STRIP_LPE
 #define STRIP_LPE 16
 #endif
+#ifndef STRIP_PROJ_LPE
+#define STRIP_PROJ_LPE 8
+#endif
 template <int OP, int MODE>
 __host__ __device__ constexpr int lanes_per_event() {
-  return (MODE == STRIP_MODE_CPU && OP != OP_GRAD) ? STRIP_LPE : 32;
+  return MODE != STRIP_MODE_CPU || OP == OP_GRAD ? 32
+         : OP == OP_MLEM                        ? STRIP_LPE
+         : STRIP_LPE == 32                      ? 32
+                                                : STRIP_PROJ_LPE;
 }
 // Row blocks a lane keeps in registers (a super-block is LPE * blocks rows).
 // MLEM keeps its rows for both passes: with half-warps 5 blocks hold the at
@@ -317,15 +324,22 @@ __host__ __device__ constexpr int lanes_per_event() {
 #ifndef STRIP_PROJ_BLOCKS
 #define STRIP_PROJ_BLOCKS 3
 #endif
+#ifndef STRIP_PROJ_BLOCKS8
+#define STRIP_PROJ_BLOCKS8 3
+#endif
+#ifndef STRIP_WHOLE_BLOCKS
+#define STRIP_WHOLE_BLOCKS 3
+#endif
 template <int OP, int LPE, bool BATCH = false>
 __host__ __device__ constexpr int row_blocks() {
-  return LPE == 32        ? 3
+  return LPE == 32        ? (OP == OP_MLEM ? STRIP_WHOLE_BLOCKS : 3)
+         : LPE == 8       ? STRIP_PROJ_BLOCKS8
          : OP != OP_MLEM  ? STRIP_PROJ_BLOCKS
          : BATCH          ? STRIP_BATCH_BLOCKS
                           : STRIP_MLEM_BLOCKS;
 }
 // Whether a launch whose tallest event box has max_rows rows gives its events
-// half-warps (where lanes_per_event allows): MLEM only when one super-block
+// fewer than 32 lanes (lanes_per_event): MLEM only when one super-block
 // holds every event, since past it pass 2 rebuilds the rows of the further
 // super-blocks (a whole warp's 96-row super-block suits taller boxes, e.g.
 // the up to 126 rows of sigma_dl = 42 mm on 1 mm pixels, better: measured
@@ -701,8 +715,8 @@ __device__ __forceinline__ EventF fetch_event(const ScannerF& s, const EventPack
 }
 
 // One event on a group of LPE lanes (every lane of the warp calls this; with
-// LPE = 16 the two half-warps bring two events, and an empty event has no
-// box rows): the event of set-up lane src (has: there is one).  Returns, in
+// LPE < 32 each group of the warp brings its own event, and an empty event
+// has no box rows): the event of set-up lane src (has: there is one).  Returns, in
 // the event's lanes, 1 / D_e for an MLEM event with a positive denominator
 // (the work item's statistic), 0 otherwise; -1 / D_e for an event the
 // unweighted window had no room for (not scattered: the caller runs it again
@@ -714,13 +728,14 @@ __device__ __forceinline__ float process_event(const LaunchArgs& a,
                                                const EventPack& mine, int src, bool has,
                                                const Win& win,
                                                int lane, const EventAux& aux) {
-  static_assert(LPE == 32 || LPE == 16, "a warp or a half-warp per event");
+  static_assert(LPE == 32 || LPE == 16 || LPE == 8, "a warp, a half or a quarter per event");
   static_assert(OP != OP_GRAD || LPE == 32, "the sigma gradient takes a warp");
   const EventF e = fetch_event(a.s, mine, src, has);
   const int sub = lane & (LPE - 1);
   const int H = (e.bry > e.tly && e.brx > e.tlx) ? e.bry - e.tly : 0;
   int Hw = H;  // the warp's largest, for loop bounds the whole warp shares
-  if constexpr (LPE < 32) Hw = max(Hw, __shfl_xor_sync(kFull, Hw, 16));
+#pragma unroll
+  for (int o = LPE; o < 32; o <<= 1) Hw = max(Hw, __shfl_xor_sync(kFull, Hw, o));
   if (Hw == 0) return 0.0f;
   const EventRows er = event_rows(a.s, e);
   if constexpr (OP == OP_GRAD) {
@@ -1031,13 +1046,15 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
 
 // CTAs per SM a tile kernel is compiled for: MLEM keeps two windows (image
 // and accumulator) and up to 64 registers a thread (2 x 16 warps per SM);
-// the GaussianKernel forward and adjoint keep one window each and fit 40
-// registers, for 3 x 16 warps.
+// the GaussianKernel forward and adjoint keep one window each; at 2 x 16
+// warps (64 registers, no spills) they ran 5 % / 1 % faster than at
+// 3 x 16 warps (40 registers, with spills) once they took a quarter-warp per
+// event.
 #ifndef STRIP_FWD_CTAS
-#define STRIP_FWD_CTAS 3
+#define STRIP_FWD_CTAS 2
 #endif
 #ifndef STRIP_ADJ_CTAS
-#define STRIP_ADJ_CTAS 3
+#define STRIP_ADJ_CTAS 2
 #endif
 template <int OP, int MODE>
 constexpr int tile_ctas_per_sm() {
@@ -1447,8 +1464,9 @@ cudaError_t launch_tile_lpe(const LaunchArgs& a, cudaStream_t st) {
 
 template <int OP, int MODE, int ACC>
 cudaError_t launch_tile_t(const LaunchArgs& a, cudaStream_t st) {
-  if constexpr (lanes_per_event<OP, MODE>() == 16) {
-    if (half_warp_events(OP, a.t.max_rows)) return launch_tile_lpe<OP, MODE, ACC, 16>(a, st);
+  constexpr int kLanes = lanes_per_event<OP, MODE>();
+  if constexpr (kLanes < 32) {
+    if (half_warp_events(OP, a.t.max_rows)) return launch_tile_lpe<OP, MODE, ACC, kLanes>(a, st);
   }
   return launch_tile_lpe<OP, MODE, ACC, 32>(a, st);
 }

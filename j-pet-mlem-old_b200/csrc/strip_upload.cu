@@ -12,6 +12,7 @@
 // finished, so the reads of one thread overlap the copies of the others.
 // The raw triples land in device memory as they are in the file, and a
 // kernel splits them into the z_u / z_d / dl arrays the binning reads.
+#include <chrono>
 #include <cuda_runtime.h>
 #include <fcntl.h>
 #include <sys/stat.h>
@@ -196,7 +197,10 @@ int upload_responses(strip_ctx* ctx, const float* t, int64_t n, int n_subsets) {
     cudaGetLastError();
     return upload_fail(ctx, STRIP_E_NOMEM, "no device memory for the events");
   }
+  const auto t0 = std::chrono::steady_clock::now();
   int rc = host_upload(ctx, t, bytes, reinterpret_cast<char*>(d_aos), "responses");
+  ctx->stats.last_upload_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (rc == STRIP_OK) rc = bin_triples(ctx, d_aos, n, n_subsets);
   cudaFree(d_aos);
   return rc;
@@ -238,6 +242,7 @@ extern "C" int strip_load_responses_file(strip_ctx* ctx, const char* path,
     return ctx_fail(ctx, STRIP_E_NOMEM, "no device memory for the events");
   }
   const off_t base = (off_t)first * 12;
+  const auto t0 = std::chrono::steady_clock::now();
   int rc = stage_upload(
       ctx, bytes, reinterpret_cast<char*>(d_aos),
       [fd, base](size_t off, size_t len, char* buf) {
@@ -252,6 +257,8 @@ extern "C" int strip_load_responses_file(strip_ctx* ctx, const char* path,
       },
       path);
   close(fd);
+  ctx->stats.last_upload_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (rc == STRIP_OK) rc = bin_triples(ctx, d_aos, count, n_subsets);
   cudaFree(d_aos);
   if (rc == STRIP_OK && n_loaded) *n_loaded = count;

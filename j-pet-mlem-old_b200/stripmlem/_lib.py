@@ -93,6 +93,7 @@ class Stats(ctypes.Structure):
         ("n_fallback", ctypes.c_int64),
         ("max_item_events", ctypes.c_int32),
         ("reserved", ctypes.c_int32),
+        ("last_upload_ms", ctypes.c_double),
     ]
 
 
