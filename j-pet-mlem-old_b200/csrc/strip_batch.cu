@@ -149,7 +149,11 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
   std::vector<BatchItem> items;
   for (int m = 0; m < n_members && rc == STRIP_OK; ++m) {
     strip_ctx* c = members[m];
+    // the persistent kernel reads row-major windows: a member binned with
+    // column-major ones is binned again
+    c->rowmajor_only = true;
     rc = ctx_prepare_mlem(c, mode);
+    if (rc == STRIP_OK && c->t.cs != 0) rc = ctx_rebin(c, c->tile_pref);
     if (rc != STRIP_OK) {
       b->err = "member " + std::to_string(m) + ": " + c->err;
       break;

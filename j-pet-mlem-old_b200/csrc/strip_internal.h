@@ -64,7 +64,10 @@ struct Tiling {
   int WXmax, WYmax, WS;
   int smem_bytes;  // the two shared-memory windows
   int max_rows;    // the most box rows of any event (the kernels' lane layout)
+  int cs;          // window column stride: kColumnStride (column-major) or 0
 };
+// Column stride of column-major tile windows (words; a multiple of 32).
+constexpr int kColumnStride = 128;
 
 __host__ __device__ inline void tile_window(const Tiling& t, int n_z, int n_y,
                                             int tile, int& wx0, int& wy0,
@@ -157,6 +160,7 @@ KernelF make_kernel(double sigma_z, double sigma_dl, float pw);
 
 // ---- launchers (strip_kernels.cu) ----------------------------------------
 int tile_smem_bytes(int WYmax, int WS);
+int tile_column_stride(int WXmax, int WYmax, int budget);
 cudaError_t launch_event_boxes(const ScannerF& s, const float* zu,
                                const float* zd, const float* dl, int64_t n,
                                int4* boxes, int* max_wh, unsigned long long* n_empty,

@@ -44,6 +44,10 @@ constexpr int kTileThreads = STRIP_TILE_THREADS;
 // run 1024-thread CTAs (32 warps, 64 registers each), so the SM keeps as
 // many resident warps as with two 512-thread CTAs.
 constexpr int kWideThreads = 1024;
+// Column-major tile windows where they fit (tile_column_stride).
+#ifndef STRIP_COLUMN_MAJOR
+#define STRIP_COLUMN_MAJOR 1
+#endif
 constexpr int kMaxWarps = kWideThreads / 32;
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -165,7 +169,16 @@ __shared__ float s_item_rsum;
 __shared__ unsigned s_fb_bits[kMaxItemEvents / 32];
 __shared__ int s_fb_n;
 
-template <int KIND>
+// A tile's window in shared memory: row-major with row stride WS (CS = 0), or
+// column-major with column stride CS words (a multiple of 32).  Column-major,
+// a lane walking its row stays in one bank, that of its row (its word
+// addresses differ by multiples of 32), so the lanes of a row block -- rows
+// of distinct banks, whatever their runs' first columns -- do not conflict;
+// row-major, a lane's bank follows its run's first column, and the lanes of
+// one instruction collide about twice as often (a bank-conflict simulation
+// over the benchmark's events: 2.39 wavefronts per walk instruction
+// row-major, 1.80 column-major).
+template <int KIND, int CS = 0>
 struct SmemWin {
   const float* w;
   float* acc;
@@ -173,16 +186,19 @@ struct SmemWin {
   float fixed_unit;
   uint32_t w_sh, acc_sh;  // shared-space addresses of w and acc
   static constexpr bool kShared = true;
+  // words between neighbouring pixels of a row, and their byte distance
+  static constexpr int kStep = CS ? CS : 1;
+  static constexpr uint32_t kPixB = 4u * kStep;
   __device__ __forceinline__ uint32_t w_addr(int p) const { return w_sh + 4u * (uint32_t)p; }
   __device__ __forceinline__ uint32_t acc_addr(int p) const { return acc_sh + 4u * (uint32_t)p; }
   __device__ __forceinline__ float unit() const {
     return KIND == kAccF32 ? 1.0f : fixed_unit;
   }
   __device__ __forceinline__ int ptr(int iy, int col) const {
-    return (iy - wy0) * WS + (col - wx0);
+    return CS ? (col - wx0) * CS + (iy - wy0) : (iy - wy0) * WS + (col - wx0);
   }
   // A lane's run of row iy kept in one register: window offset << 16 | len
-  // (windows hold < 2^15 pixels, runs < 2^16).
+  // (windows hold < 2^16 words, runs < 2^16).
   __device__ __forceinline__ unsigned pack_run(int iy, int lo, int len) const {
     return len > 0 ? ((unsigned)ptr(iy, lo) << 16) | (unsigned)len : 0u;
   }
@@ -190,21 +206,21 @@ struct SmemWin {
                                          int) const {
     return (int)(v >> 16);
   }
-  __device__ __forceinline__ float read(int p, int j) const { return w[p + j]; }
+  __device__ __forceinline__ float read(int p, int j) const { return w[p + j * kStep]; }
   // acc_j += v (v already scaled by unit())
   __device__ __forceinline__ void add(int p, int j, float v) const {
     if constexpr (KIND == kAccS32)
-      atomicAdd(reinterpret_cast<int*>(acc) + p + j,
+      atomicAdd(reinterpret_cast<int*>(acc) + p + j * kStep,
                 (int)(__float_as_uint(v + kMagicSigned) - kMagicSignedBits));
     else
-      atomicAdd(acc + p + j, v);
+      atomicAdd(acc + p + j * kStep, v);
   }
   // acc_j += K_j w_j / D_e for K_j = E * pref and sc = pref / D_e * unit()
   __device__ __forceinline__ void add_weighted(int p, int j, float E,
                                                float sc) const {
-    const unsigned v = KIND == kAccU32Cvt ? __float2uint_rn(E * w[p + j] * sc)
-                                          : to_fixed(E * w[p + j], sc);
-    atomicAdd(reinterpret_cast<unsigned*>(acc) + p + j, v);
+    const unsigned v = KIND == kAccU32Cvt ? __float2uint_rn(E * w[p + j * kStep] * sc)
+                                          : to_fixed(E * w[p + j * kStep], sc);
+    atomicAdd(reinterpret_cast<unsigned*>(acc) + p + j * kStep, v);
   }
   // signed fixed point: the adjoint's pair walk adds two pixels a step
   __host__ __device__ static constexpr bool pair_add() { return KIND == kAccS32; }
@@ -473,8 +489,8 @@ __device__ __forceinline__ void pass1_rows(const ScannerF& s, const KernelF& k,
         float2 A = make_float2(0.0f, 0.0f);
         uint32_t ad = win.w_addr(p);
 #pragma unroll 2
-        for (int c = n >> 1; c > 0; --c, ad += 8) {
-          A = __ffma2_rn(P, make_float2(lds32(ad), lds32(ad + 4)), A);
+        for (int c = n >> 1; c > 0; --c, ad += 2 * Win::kPixB) {
+          A = __ffma2_rn(P, make_float2(lds32(ad), lds32(ad + Win::kPixB)), A);
           P = __fmul2_rn(P, S);
           S = __fmul2_rn(S, Q4);
         }
@@ -543,9 +559,9 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
         const float2 Q4 = make_float2(k.q4, k.q4);
         uint32_t aa = win.acc_addr(p);
 #pragma unroll 2
-        for (int c = n >> 1; c > 0; --c, aa += 8) {
+        for (int c = n >> 1; c > 0; --c, aa += 2 * Win::kPixB) {
           red_shared_add(aa, __float2uint_rn(P.x));
-          red_shared_add(aa + 4, __float2uint_rn(P.y));
+          red_shared_add(aa + Win::kPixB, __float2uint_rn(P.y));
           P = __fmul2_rn(P, S);
           S = __fmul2_rn(S, Q4);
         }
@@ -561,8 +577,8 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
         const float2 Q4 = make_float2(k.q4, k.q4);
         uint32_t ad = win.w_addr(p), aa = win.acc_addr(p);
 #pragma unroll 2
-        for (int c = n >> 1; c > 0; --c, ad += 8, aa += 8) {
-          const float2 w2 = make_float2(lds32(ad), lds32(ad + 4));
+        for (int c = n >> 1; c > 0; --c, ad += 2 * Win::kPixB, aa += 2 * Win::kPixB) {
+          const float2 w2 = make_float2(lds32(ad), lds32(ad + Win::kPixB));
           unsigned v0, v1;
           if constexpr (Win::fine()) {
             const float2 x = __fmul2_rn(P, w2);
@@ -574,7 +590,7 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
             v1 = __float_as_uint(x.y) - kMagicBits;
           }
           red_shared_add(aa, v0);
-          red_shared_add(aa + 4, v1);
+          red_shared_add(aa + Win::kPixB, v1);
           P = __fmul2_rn(P, S);
           S = __fmul2_rn(S, Q4);
         }
@@ -601,10 +617,10 @@ __device__ __forceinline__ void pass2_rows(const ScannerF& s, const KernelF& k,
         const float2 Q4 = make_float2(k.q4, k.q4);
         uint32_t aa = win.acc_addr(p);
 #pragma unroll 2
-        for (int c = n >> 1; c > 0; --c, aa += 8) {
+        for (int c = n >> 1; c > 0; --c, aa += 2 * Win::kPixB) {
           const float2 x = __fadd2_rn(P, make_float2(kMagicSigned, kMagicSigned));
           red_shared_add(aa, __float_as_uint(x.x) - kMagicSignedBits);
-          red_shared_add(aa + 4, __float_as_uint(x.y) - kMagicSignedBits);
+          red_shared_add(aa + Win::kPixB, __float_as_uint(x.y) - kMagicSignedBits);
           P = __fmul2_rn(P, S);
           S = __fmul2_rn(S, Q4);
         }
@@ -917,7 +933,7 @@ __device__ __forceinline__ float block_sum(float v) {
 // `index` is the item's index among the launch's items (its statistic in
 // a.item_hist).  The CTA may run further items afterwards (the batched
 // kernel): the caller synchronises before the shared memory is reused.
-template <int OP, int MODE, int ACC, int LPE, int NB>
+template <int OP, int MODE, int ACC, int LPE, int NB, int CS>
 __device__ __forceinline__ void tile_item(const LaunchArgs& a,
                                           const WorkItem it, int index,
                                           char* smem_raw, int* s_next_group) {
@@ -926,7 +942,7 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
   const int wxn = wx1 - wx0, wyn = wy1 - wy0, WS = a.t.WS;
   float* s_w = reinterpret_cast<float*>(smem_raw);
   // the adjoint reads no image: its accumulator is the only window
-  float* s_acc = OP == OP_ADJOINT ? s_w : s_w + a.t.WYmax * WS;
+  float* s_acc = OP == OP_ADJOINT ? s_w : s_w + (CS ? a.t.WXmax * CS : a.t.WYmax * WS);
   constexpr bool kReads = (OP != OP_ADJOINT);
   constexpr bool kWrites = (OP == OP_MLEM || OP == OP_ADJOINT);
   constexpr bool kFixedMlem = (OP == OP_MLEM && MODE == STRIP_MODE_CPU);
@@ -940,16 +956,18 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
     for (int q = threadIdx.x; q < kMaxItemEvents / 32; q += blockDim.x) s_fb_bits[q] = 0u;
   const int lane = threadIdx.x & 31;
   float wsum = 0.0f;
+  // window word of (row r, column c): row-major or column-major (CS)
+  auto widx = [WS](int r, int c) { return CS ? c * CS + r : r * WS + c; };
   for (int q = threadIdx.x; q < wxn * wyn; q += blockDim.x) {
     const int r = q / wxn, c = q - r * wxn;
     const int64_t gi = (int64_t)(wy0 + r) * a.s.n_z + wx0 + c;
     if (kReads) {
       float v = a.rho[gi];
       if (MODE == STRIP_MODE_GPU) v *= a.sens[gi];
-      s_w[r * WS + c] = v;
+      s_w[widx(r, c)] = v;
       wsum += v;
     }
-    if (kWrites) s_acc[r * WS + c] = 0.0f;
+    if (kWrites) s_acc[widx(r, c)] = 0.0f;
   }
   __syncthreads();
   const uint32_t w_sh = (uint32_t)__cvta_generic_to_shared(s_w);
@@ -963,16 +981,17 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
     for (int q = threadIdx.x; q < wxn * wyn; q += blockDim.x) {
       const int r = q / wxn, c = q - r * wxn;
       double v;
+      const int wi = widx(r, c);
       if constexpr (kFixedMlem) {
-        v = ldexp((double)s_acc_u[r * WS + c], -fshift);
+        v = ldexp((double)s_acc_u[wi], -fshift);
         if (unweighted) {
-          v *= (double)s_w[r * WS + c];
-          s_acc_u[r * WS + c] = 0u;
+          v *= (double)s_w[wi];
+          s_acc_u[wi] = 0u;
         }
       } else if constexpr (OP == OP_ADJOINT && MODE == STRIP_MODE_CPU) {
-        v = ldexp((double)s_acc_i[r * WS + c], -fshift);
+        v = ldexp((double)s_acc_i[wi], -fshift);
       } else {
-        v = (double)s_acc[r * WS + c];
+        v = (double)s_acc[wi];
       }
       if (v != 0.0)
         atomicAdd(a.acc + (int64_t)(wy0 + r) * a.s.n_z + wx0 + c, v);
@@ -983,7 +1002,7 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
   auto run_weighted = [&](int count, const unsigned* only) {
     const int fs = fixed_shift(count);
     run_item<OP, MODE, ACC, LPE, NB>(
-        a, it, SmemWin<kAccU32Cvt>{s_w, s_acc, wx0, wy0, WS, exp2f((float)fs), w_sh, acc_sh},
+        a, it, SmemWin<kAccU32Cvt, CS>{s_w, s_acc, wx0, wy0, WS, exp2f((float)fs), w_sh, acc_sh},
         lane, s_next_group, only);
     return fs;
   };
@@ -1003,7 +1022,7 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
     if (unweighted) {
       run_item<OP, MODE, ACC, LPE, NB>(
           a, it,
-          SmemWin<kAccU32Unw>{s_w, s_acc, wx0, wy0, WS, exp2f((float)fshift), w_sh, acc_sh},
+          SmemWin<kAccU32Unw, CS>{s_w, s_acc, wx0, wy0, WS, exp2f((float)fshift), w_sh, acc_sh},
           lane, s_next_group);
       __syncthreads();
       flush(fshift, true);
@@ -1029,13 +1048,13 @@ __device__ __forceinline__ void tile_item(const LaunchArgs& a,
     const int fshift = adjoint_shift(a, it, lane);
     run_item<OP, MODE, ACC, LPE, NB>(
         a, it,
-        SmemWin<kAccS32>{s_w, s_acc, wx0, wy0, WS, exp2f((float)fshift), w_sh, acc_sh},
+        SmemWin<kAccS32, CS>{s_w, s_acc, wx0, wy0, WS, exp2f((float)fshift), w_sh, acc_sh},
         lane, s_next_group);
     __syncthreads();
     flush(fshift, false);
   } else {
     run_item<OP, MODE, ACC, LPE, NB>(a, it,
-                            SmemWin<kAccF32>{s_w, s_acc, wx0, wy0, WS, 1.0f, w_sh, acc_sh},
+                            SmemWin<kAccF32, CS>{s_w, s_acc, wx0, wy0, WS, 1.0f, w_sh, acc_sh},
                             lane, s_next_group);
     if (kWrites) {
       __syncthreads();
@@ -1066,15 +1085,15 @@ constexpr int tile_ctas_per_sm() {
 template <int OP>
 constexpr int tile_windows() { return OP == OP_MLEM ? 2 : 1; }
 
-template <int OP, int MODE, int ACC, int THREADS, int LPE>
+template <int OP, int MODE, int ACC, int THREADS, int LPE, int CS>
 __global__ void __launch_bounds__(THREADS, THREADS == kWideThreads
                                                ? 1
                                                : tile_ctas_per_sm<OP, MODE>())
     k_tile(const __grid_constant__ LaunchArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   __shared__ int s_next_group;
-  tile_item<OP, MODE, ACC, LPE, row_blocks<OP, LPE>()>(a, a.items[blockIdx.x], blockIdx.x,
-                                                       smem_raw, &s_next_group);
+  tile_item<OP, MODE, ACC, LPE, row_blocks<OP, LPE>(), CS>(a, a.items[blockIdx.x], blockIdx.x,
+                                                           smem_raw, &s_next_group);
 }
 
 // Persistent tile kernel over the work items of several reconstructions: a
@@ -1093,7 +1112,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == kWideThreads ? 1 : 2)
     const int i = s_item;
     if (i >= n_items) break;
     const BatchItem bi = items[i];
-    tile_item<OP_MLEM, MODE, ACC, LPE, row_blocks<OP_MLEM, LPE, true>()>(b.member[bi.member],
+    tile_item<OP_MLEM, MODE, ACC, LPE, row_blocks<OP_MLEM, LPE, true>(), 0>(b.member[bi.member],
                                   WorkItem{bi.tile, bi.count, bi.begin},
                                   bi.index, smem_raw, &s_next_group);
     __syncthreads();  // before the next item's window overwrites this one
@@ -1453,8 +1472,11 @@ template <int OP, int MODE, int ACC, int LPE>
 cudaError_t launch_tile_lpe(const LaunchArgs& a, cudaStream_t st) {
   const int smem = a.t.smem_bytes / 2 * tile_windows<OP>();
   const bool wide = smem > kNarrowSmemBytes;  // one CTA per SM: 1024 threads
-  auto fn = wide ? k_tile<OP, MODE, ACC, kWideThreads, LPE>
-                 : k_tile<OP, MODE, ACC, kTileThreads, LPE>;
+  auto fn = a.t.cs == kColumnStride
+                ? (wide ? k_tile<OP, MODE, ACC, kWideThreads, LPE, kColumnStride>
+                        : k_tile<OP, MODE, ACC, kTileThreads, LPE, kColumnStride>)
+                : (wide ? k_tile<OP, MODE, ACC, kWideThreads, LPE, 0>
+                        : k_tile<OP, MODE, ACC, kTileThreads, LPE, 0>);
   cudaError_t err = cudaFuncSetAttribute(
       fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (err != cudaSuccess) return err;
@@ -1498,6 +1520,14 @@ cudaError_t launch_global_t(const LaunchArgs& a, cudaStream_t st) {
 
 // Two windows (the image and the accumulator) of WYmax rows of stride WS.
 int tile_smem_bytes(int WYmax, int WS) { return 2 * WYmax * WS * 4; }
+
+// The column stride of a tiling's windows: kColumnStride (column-major) when
+// the windows are at most that many rows high and their column-major form
+// fits `budget` bytes, else 0 (row-major).
+int tile_column_stride(int WXmax, int WYmax, int budget) {
+  if (!STRIP_COLUMN_MAJOR) return 0;
+  return WYmax <= kColumnStride && 2 * WXmax * kColumnStride * 4 <= budget ? kColumnStride : 0;
+}
 
 cudaError_t launch_tile(int op, int mode, int accum, const LaunchArgs& a,
                         cudaStream_t st) {
