@@ -28,6 +28,9 @@ using namespace stripmlem;
 
 // Windows up to this size let two CTAs share an SM.
 constexpr int kNarrowSmem = kNarrowSmemBytes;
+// Work-item classes: narrow / wide windows, row-major / column-major.
+constexpr int kClasses = 4;
+inline int class_stride(int c) { return (c & 2) ? kColumnStride : 0; }
 
 struct strip_batch {
   int device = 0;
@@ -38,14 +41,15 @@ struct strip_batch {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   BatchArgs* args = nullptr;  // host copy of the kernel parameters (~20 KB)
-  // Work items in two shared-memory classes: members whose windows fit two
-  // CTAs per SM, and wide-window members (one CTA per SM).  Each class is one
+  // Work items in four classes: members whose windows fit two CTAs per SM
+  // and wide-window members (one CTA per SM), each with row-major or
+  // column-major windows (class = wide + 2 * column-major).  Each class is one
   // persistent launch, so a wide member does not halve the occupancy of the
   // others.  Class c owns items [cls_begin[c], cls_begin[c] + cls_count[c]).
   BatchItem* d_items = nullptr;
   int n_items = 0;
-  int cls_begin[2] = {0, 0}, cls_count[2] = {0, 0}, cls_smem[2] = {0, 0};
-  int cls_rows[2] = {0, 0};  // the most box rows of a class's events
+  int cls_begin[kClasses] = {}, cls_count[kClasses] = {}, cls_smem[kClasses] = {};
+  int cls_rows[kClasses] = {};  // the most box rows of a class's events
   int* d_counter = nullptr;  // one counter per class
   int64_t n_events = 0;
   int launches_per_step = 0;
@@ -89,13 +93,13 @@ void release(strip_batch* b) {
 // One step on the batch stream: counter reset, the persistent tile launch,
 // the members' global-path launches, the batched update.
 int enqueue_step(strip_batch* b) {
-  BCK(cudaMemsetAsync(b->d_counter, 0, 2 * sizeof(int), b->stream));
-  for (int c = 0; c < 2; ++c)
+  BCK(cudaMemsetAsync(b->d_counter, 0, kClasses * sizeof(int), b->stream));
+  for (int c = 0; c < kClasses; ++c)
     if (b->cls_count[c] > 0)
       BCK(launch_tile_batch(b->mode, b->accum, *b->args,
                             b->d_items + b->cls_begin[c], b->cls_count[c],
                             b->d_counter + c, b->cls_smem[c], b->cls_rows[c],
-                            b->sm_count, b->stream));
+                            class_stride(c), b->sm_count, b->stream));
   BatchUpdateArgs u{};
   u.n = (int)b->members.size();
   u.weighted = mlem_weighted(b->mode);
@@ -149,17 +153,13 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
   std::vector<BatchItem> items;
   for (int m = 0; m < n_members && rc == STRIP_OK; ++m) {
     strip_ctx* c = members[m];
-    // the persistent kernel reads row-major windows: a member binned with
-    // column-major ones is binned again
-    c->rowmajor_only = true;
     rc = ctx_prepare_mlem(c, mode);
-    if (rc == STRIP_OK && c->t.cs != 0) rc = ctx_rebin(c, c->tile_pref);
     if (rc != STRIP_OK) {
       b->err = "member " + std::to_string(m) + ": " + c->err;
       break;
     }
     b->args->member[m] = ctx_mlem_args(c, mode);
-    const int cls = c->t.smem_bytes > kNarrowSmem;
+    const int cls = (c->t.smem_bytes > kNarrowSmem) + (c->t.cs != 0 ? 2 : 0);
     b->cls_smem[cls] = std::max(b->cls_smem[cls], c->t.smem_bytes);
     b->cls_rows[cls] = std::max(b->cls_rows[cls], c->t.max_rows);
     b->n_events += c->n_events;
@@ -178,8 +178,9 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
                      });
     b->n_items = (int)items.size();
     for (const BatchItem& it : items) ++b->cls_count[it.pad];
-    b->cls_begin[1] = b->cls_count[0];
-    b->launches_per_step += 1 + (b->cls_count[0] > 0) + (b->cls_count[1] > 0);
+    for (int c = 1; c < kClasses; ++c) b->cls_begin[c] = b->cls_begin[c - 1] + b->cls_count[c - 1];
+    b->launches_per_step += 1;
+    for (int c = 0; c < kClasses; ++c) b->launches_per_step += b->cls_count[c] > 0;
     do {
       if (cudaSetDevice(b->device) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
       if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
@@ -188,7 +189,7 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
         break;
       }
       if (cudaMalloc(&b->d_items, std::max<size_t>(items.size(), 1) * sizeof(BatchItem)) != cudaSuccess ||
-          cudaMalloc(&b->d_counter, 2 * sizeof(int)) != cudaSuccess) {
+          cudaMalloc(&b->d_counter, kClasses * sizeof(int)) != cudaSuccess) {
         rc = STRIP_E_NOMEM;
         break;
       }
@@ -204,12 +205,12 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
       if (rc != STRIP_OK) break;
       // capture one step as a graph (kernel attributes are set beforehand)
       // (each class has its own kernel: 512-thread CTAs for the narrow
-      // windows, 1024-thread CTAs for the wide ones)
+      // windows, 1024-thread CTAs for the wide ones, per window layout)
       bool attr_ok = true;
-      for (int c = 0; c < 2; ++c)
+      for (int c = 0; c < kClasses; ++c)
         if (b->cls_count[c] > 0 &&
-            tile_batch_reserve_smem(b->mode, b->accum, b->cls_smem[c], b->cls_rows[c]) !=
-                cudaSuccess)
+            tile_batch_reserve_smem(b->mode, b->accum, b->cls_smem[c], b->cls_rows[c],
+                                    class_stride(c)) != cudaSuccess)
           attr_ok = false;
       if (!attr_ok ||
           cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {

@@ -166,8 +166,8 @@ Tiling choose_tiling(const strip_ctx* ctx, int max_w, int max_h) {
     if (HX >= HY) HX = HX * 3 / 4; else HY = HY * 3 / 4;
   }
   // column-major windows where they fit the same budget (fewer shared-memory
-  // bank conflicts in the walks); never for the members of a persistent batch
-  t.cs = ctx->rowmajor_only ? 0 : tile_column_stride(t.WXmax, t.WYmax, budget);
+  // bank conflicts in the walks)
+  t.cs = tile_column_stride(t.WXmax, t.WYmax, budget);
   if (t.cs) t.smem_bytes = 2 * t.WXmax * t.cs * 4;
   t.ntx = (n_z + t.TX - 1) / t.TX;
   t.nty = (n_y + t.TY - 1) / t.TY;

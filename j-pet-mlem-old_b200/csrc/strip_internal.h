@@ -195,11 +195,13 @@ cudaError_t launch_gather_weights(const int64_t* perm, const double* w,
                                   int64_t n, float* out, cudaStream_t st);
 // Sets the batched tile kernel's dynamic shared-memory limit (before a
 // launch is captured into a graph).
-// max_rows: the most box rows of any event of the launch's members.
-cudaError_t tile_batch_reserve_smem(int mode, int accum, int smem_bytes, int max_rows);
+// max_rows: the most box rows of any event of the launch's members; cs:
+// their windows' column stride (0: row-major).
+cudaError_t tile_batch_reserve_smem(int mode, int accum, int smem_bytes, int max_rows, int cs);
 cudaError_t launch_tile_batch(int mode, int accum, const BatchArgs& b,
                               const BatchItem* items, int n_items, int* counter,
-                              int smem_bytes, int max_rows, int sm_count, cudaStream_t st);
+                              int smem_bytes, int max_rows, int cs, int sm_count,
+                              cudaStream_t st);
 cudaError_t launch_update_batch(const BatchUpdateArgs& u, int64_t max_pix,
                                 cudaStream_t st);
 cudaError_t launch_sensitivity(const ScannerF& s, int five_point, float* out,

@@ -1099,7 +1099,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == kWideThreads
 // Persistent tile kernel over the work items of several reconstructions: a
 // CTA takes item after item from a global counter; item i belongs to member
 // items[i].member, whose arguments live in the kernel's parameter space.
-template <int MODE, int ACC, int THREADS, int LPE>
+template <int MODE, int ACC, int THREADS, int LPE, int CS>
 __global__ void __launch_bounds__(THREADS, THREADS == kWideThreads ? 1 : 2)
     k_tile_batch(const __grid_constant__ BatchArgs b, const BatchItem* items,
                  int n_items, int* counter) {
@@ -1112,7 +1112,7 @@ __global__ void __launch_bounds__(THREADS, THREADS == kWideThreads ? 1 : 2)
     const int i = s_item;
     if (i >= n_items) break;
     const BatchItem bi = items[i];
-    tile_item<OP_MLEM, MODE, ACC, LPE, row_blocks<OP_MLEM, LPE, true>(), 0>(b.member[bi.member],
+    tile_item<OP_MLEM, MODE, ACC, LPE, row_blocks<OP_MLEM, LPE, true>(), CS>(b.member[bi.member],
                                   WorkItem{bi.tile, bi.count, bi.begin},
                                   bi.index, smem_raw, &s_next_group);
     __syncthreads();  // before the next item's window overwrites this one
@@ -1565,43 +1565,48 @@ cudaError_t launch_global(int op, int mode, int accum, const LaunchArgs& a,
   }
 }
 
-template <int THREADS, class F>
+template <int THREADS, int CS, class F>
 cudaError_t with_tile_batch_t(int mode, int accum, bool half, F&& pick) {
   if (mode == STRIP_MODE_CPU) {
     constexpr int H = lanes_per_event<OP_MLEM, STRIP_MODE_CPU>();
     if (half) {
       if (accum == STRIP_ACCUM_FP32)
-        return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP32, THREADS, H>);
+        return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP32, THREADS, H, CS>);
       if (accum == STRIP_ACCUM_FP64)
-        return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP64, THREADS, H>);
-      return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_KAHAN, THREADS, H>);
+        return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP64, THREADS, H, CS>);
+      return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_KAHAN, THREADS, H, CS>);
     }
     if (accum == STRIP_ACCUM_FP32)
-      return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP32, THREADS, 32>);
+      return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP32, THREADS, 32, CS>);
     if (accum == STRIP_ACCUM_FP64)
-      return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP64, THREADS, 32>);
-    return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_KAHAN, THREADS, 32>);
+      return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_FP64, THREADS, 32, CS>);
+    return pick(k_tile_batch<STRIP_MODE_CPU, STRIP_ACCUM_KAHAN, THREADS, 32, CS>);
   }
   if (accum == STRIP_ACCUM_FP32)
-    return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_FP32, THREADS, 32>);
+    return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_FP32, THREADS, 32, CS>);
   if (accum == STRIP_ACCUM_FP64)
-    return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_FP64, THREADS, 32>);
-  return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_KAHAN, THREADS, 32>);
+    return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_FP64, THREADS, 32, CS>);
+  return pick(k_tile_batch<STRIP_MODE_GPU, STRIP_ACCUM_KAHAN, THREADS, 32, CS>);
 }
 
-// The persistent batch kernel of a shared-memory class: windows that fit two
-// CTAs per SM run 512-thread CTAs, wider ones 1024-thread CTAs, one per SM;
-// half-warp events where every member's tallest box allows them.
+// The persistent batch kernel of a class: windows that fit two CTAs per SM
+// run 512-thread CTAs, wider ones 1024-thread CTAs, one per SM; half-warp
+// events where every member's tallest box allows them; row-major or
+// column-major windows (cs).
 template <class F>
-cudaError_t with_tile_batch(int mode, int accum, int smem_bytes, int max_rows, F&& pick) {
+cudaError_t with_tile_batch(int mode, int accum, int smem_bytes, int max_rows, int cs,
+                            F&& pick) {
   const bool half = half_warp_events(OP_MLEM, max_rows, true);
-  if (smem_bytes > kNarrowSmemBytes)
-    return with_tile_batch_t<kWideThreads>(mode, accum, half, pick);
-  return with_tile_batch_t<kTileThreads>(mode, accum, half, pick);
+  const bool wide = smem_bytes > kNarrowSmemBytes;
+  if (cs == kColumnStride)
+    return wide ? with_tile_batch_t<kWideThreads, kColumnStride>(mode, accum, half, pick)
+                : with_tile_batch_t<kTileThreads, kColumnStride>(mode, accum, half, pick);
+  return wide ? with_tile_batch_t<kWideThreads, 0>(mode, accum, half, pick)
+              : with_tile_batch_t<kTileThreads, 0>(mode, accum, half, pick);
 }
 
-cudaError_t tile_batch_reserve_smem(int mode, int accum, int smem_bytes, int max_rows) {
-  return with_tile_batch(mode, accum, smem_bytes, max_rows, [&](auto fn) {
+cudaError_t tile_batch_reserve_smem(int mode, int accum, int smem_bytes, int max_rows, int cs) {
+  return with_tile_batch(mode, accum, smem_bytes, max_rows, cs, [&](auto fn) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 smem_bytes);
   });
@@ -1609,7 +1614,8 @@ cudaError_t tile_batch_reserve_smem(int mode, int accum, int smem_bytes, int max
 
 cudaError_t launch_tile_batch(int mode, int accum, const BatchArgs& b,
                               const BatchItem* items, int n_items, int* counter,
-                              int smem_bytes, int max_rows, int sm_count, cudaStream_t st) {
+                              int smem_bytes, int max_rows, int cs, int sm_count,
+                              cudaStream_t st) {
   if (n_items <= 0) return cudaSuccess;
   const bool wide = smem_bytes > kNarrowSmemBytes;
   auto pick = [&](auto fn) -> cudaError_t {
@@ -1617,7 +1623,7 @@ cudaError_t launch_tile_batch(int mode, int accum, const BatchArgs& b,
     fn<<<grid, wide ? kWideThreads : kTileThreads, smem_bytes, st>>>(b, items, n_items, counter);
     return cudaGetLastError();
   };
-  return with_tile_batch(mode, accum, smem_bytes, max_rows, pick);
+  return with_tile_batch(mode, accum, smem_bytes, max_rows, cs, pick);
 }
 
 
