@@ -107,6 +107,12 @@ KernelF make_kernel(double sigma_z, double sigma_dl, float pw) {
 
 }  // namespace stripmlem
 
+// Each work item's events ordered for the column-major windows' banks
+// (k_item_order; a build-time switch for comparisons).
+#ifndef STRIP_ITEM_ORDER
+#define STRIP_ITEM_ORDER 1
+#endif
+
 namespace {
 
 template <class T>
@@ -311,6 +317,37 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
       cudaFree(d_ihist);
       CKB(e);
     }
+  }
+  // column-major windows: each item's events in quads of middle-row classes
+  // (k_item_order); the binned arrays are replaced by the ordered ones
+  if (t.cs != 0 && !items.empty() && STRIP_ITEM_ORDER) {
+    float *qzu = nullptr, *qzd = nullptr, *qdl = nullptr;
+    int64_t* qperm = nullptr;
+    cudaError_t e = cudaMalloc(&qzu, nb * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&qzd, nb * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&qdl, nb * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&qperm, nb * sizeof(int64_t));
+    if (e == cudaSuccess)
+      e = launch_item_order(ctx->s, t, d_items, (int)items.size(), ozu, ozd, odl, operm, qzu,
+                            qzd, qdl, qperm, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      cudaFree(qzu);
+      cudaFree(qzd);
+      cudaFree(qdl);
+      cudaFree(qperm);
+      cudaFree(d_items);
+      cudaFree(d_ihist);
+      CKB(e);
+    }
+    std::swap(ozu, qzu);
+    std::swap(ozd, qzd);
+    std::swap(odl, qdl);
+    std::swap(operm, qperm);
+    cudaFree(qzu);
+    cudaFree(qzd);
+    cudaFree(qdl);
+    cudaFree(qperm);
   }
   cudaEventRecord(ctx->ev1, st);
   {

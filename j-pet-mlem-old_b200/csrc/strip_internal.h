@@ -177,6 +177,12 @@ cudaError_t launch_bin_scatter(const int* keys, int64_t n, const float* zu,
                                int64_t n_keys, cudaStream_t st);
 cudaError_t launch_tile(int op, int mode, int accum, const LaunchArgs& a,
                         cudaStream_t st);
+// The events of each work item (binned arrays zu.. perm) reordered into
+// ozu.. operm for the column-major windows' banks (k_item_order).
+cudaError_t launch_item_order(const ScannerF& s, const Tiling& t, const WorkItem* items,
+                              int n_items, const float* zu, const float* zd, const float* dl,
+                              const int64_t* perm, float* ozu, float* ozd, float* odl,
+                              int64_t* operm, cudaStream_t st);
 cudaError_t launch_global(int op, int mode, int accum, const LaunchArgs& a,
                           cudaStream_t st);
 // rho_j <- rho_j * acc_j * scale, or acc_j * scale when the accumulator holds

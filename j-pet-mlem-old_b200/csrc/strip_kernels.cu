@@ -1317,6 +1317,83 @@ __global__ void k_bin_scatter(const int* keys, int64_t n, const float* zu,
   }
 }
 
+// Orders the events of each work item for the column-major windows' banks.
+// A lane's bank there is its row's, (row - wy0) mod 32, and the rows of a
+// row block, ranked middle-out from the event's middle row m, cover a fixed
+// set of residues around m: for 16-row blocks half of Z_32 whose other half
+// is the same set around m + 16, for 8-row blocks a quarter whose shifts by
+// 8, 16 and 24 tile Z_32.  So the item is laid out in quads of events whose
+// middle rows are v, v + 16, v + 8 and v + 24 mod 32 (the half-warp pairs of
+// MLEM take (v, v + 16) and (v + 8, v + 24), the quarter-warps of the
+// forward and adjoint all four), then pairs (v, v + 16) of the events left,
+// then the rest.  One CTA per item; the order within a middle-row class is
+// that of the atomics.  The results change only by the order of the binary32
+// sums.
+__global__ void k_item_order(ScannerF s, Tiling t, const WorkItem* __restrict__ items,
+                             const float* __restrict__ zu, const float* __restrict__ zd,
+                             const float* __restrict__ dl, const int64_t* __restrict__ perm,
+                             float* ozu, float* ozd, float* odl, int64_t* operm) {
+  __shared__ int s_n[32], s_cnt[32];
+  __shared__ int s_q[32], s_qbase[32], s_p[32], s_pbase[32], s_sbase[32];
+  const WorkItem it = items[blockIdx.x];
+  int wx0, wy0, wx1, wy1;
+  tile_window(t, s.n_z, s.n_y, it.tile, wx0, wy0, wx1, wy1);
+  if (threadIdx.x < 32) {
+    s_n[threadIdx.x] = 0;
+    s_cnt[threadIdx.x] = 0;
+  }
+  __syncthreads();
+  auto cls = [&](int64_t i) {
+    EventF e;
+    event_setup(s, zu[i], zd[i], dl[i], e);
+    return (e.tly + ((e.bry - e.tly - 1) >> 1) - wy0) & 31;
+  };
+  for (int k = threadIdx.x; k < it.count; k += blockDim.x) atomicAdd(&s_n[cls(it.begin + k)], 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int left[32];
+    for (int v = 0; v < 32; ++v) left[v] = s_n[v];
+    int pos = 0;
+    for (int v = 0; v < 8; ++v) {  // quads: v, v + 16, v + 8, v + 24
+      const int c[4] = {v, v + 16, v + 8, v + 24};
+      const int q = min(min(left[c[0]], left[c[1]]), min(left[c[2]], left[c[3]]));
+      for (int j = 0; j < 4; ++j) {
+        s_q[c[j]] = q;
+        s_qbase[c[j]] = pos + j;
+        left[c[j]] -= q;
+      }
+      pos += 4 * q;
+    }
+    for (int v = 0; v < 16; ++v) {  // pairs: v, v + 16
+      const int p = min(left[v], left[v + 16]);
+      s_p[v] = s_p[v + 16] = p;
+      s_pbase[v] = pos;
+      s_pbase[v + 16] = pos + 1;
+      left[v] -= p;
+      left[v + 16] -= p;
+      pos += 2 * p;
+    }
+    for (int v = 0; v < 32; ++v) {  // the rest
+      s_sbase[v] = pos;
+      pos += left[v];
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < it.count; k += blockDim.x) {
+    const int64_t i = it.begin + k;
+    const int v = cls(i);
+    const int r = atomicAdd(&s_cnt[v], 1);
+    const int q = s_q[v], p = s_p[v];
+    const int at = r < q ? s_qbase[v] + 4 * r
+                         : r < q + p ? s_pbase[v] + 2 * (r - q) : s_sbase[v] + (r - q - p);
+    const int64_t o = it.begin + at;
+    ozu[o] = zu[i];
+    ozd[o] = zd[i];
+    odl[o] = dl[i];
+    operm[o] = perm[i];
+  }
+}
+
 __global__ void k_gather_weights(const int64_t* perm, const double* w,
                                  int64_t n, float* out) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -1682,6 +1759,15 @@ cudaError_t launch_update(float* rho, double* acc, int64_t n_pix, double scale,
                           int weighted, cudaStream_t st) {
   k_update<<<grid_for(n_pix), kThreads, 0, st>>>(rho, acc, n_pix, scale,
                                                  weighted);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_item_order(const ScannerF& s, const Tiling& t, const WorkItem* items,
+                              int n_items, const float* zu, const float* zd, const float* dl,
+                              const int64_t* perm, float* ozu, float* ozd, float* odl,
+                              int64_t* operm, cudaStream_t st) {
+  if (n_items <= 0) return cudaSuccess;
+  k_item_order<<<n_items, 256, 0, st>>>(s, t, items, zu, zd, dl, perm, ozu, ozd, odl, operm);
   return cudaGetLastError();
 }
 
