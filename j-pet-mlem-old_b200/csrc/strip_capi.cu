@@ -197,15 +197,15 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
   float *ozu = nullptr, *ozd = nullptr, *odl = nullptr;
   int64_t* operm = nullptr;
   auto cleanup = [&]() {
-    dfree(boxes);
-    dfree(keys);
+    ev_free(ctx, boxes);
+    ev_free(ctx, keys);
     dfree(d_wh);
     dfree(d_empty);
     dfree(d_hist);
-    dfree(ozu);
-    dfree(ozd);
-    dfree(odl);
-    dfree(operm);
+    ev_free(ctx, ozu);
+    ev_free(ctx, ozd);
+    ev_free(ctx, odl);
+    ev_free(ctx, operm);
   };
   int rc = STRIP_OK;
 #define CKB(call)                                                        \
@@ -220,8 +220,8 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
     }                                                                    \
   } while (0)
   const size_t nn = (size_t)std::max<int64_t>(n, 1);
-  CKB(cudaMalloc(&boxes, nn * sizeof(int4)));
-  CKB(cudaMalloc(&keys, nn * sizeof(int)));
+  CKB(ev_alloc(ctx, &boxes, nn * sizeof(int4)));
+  CKB(ev_alloc(ctx, &keys, nn * sizeof(int)));
   CKB(cudaMalloc(&d_wh, 2 * sizeof(int)));
   CKB(cudaMalloc(&d_empty, sizeof(unsigned long long)));
   CKB(cudaMemsetAsync(d_wh, 0, 2 * sizeof(int), st));
@@ -252,10 +252,10 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
     total += hist[k];
   }
   const size_t nb = (size_t)std::max<unsigned long long>(total, 1);
-  CKB(cudaMalloc(&ozu, nb * sizeof(float)));
-  CKB(cudaMalloc(&ozd, nb * sizeof(float)));
-  CKB(cudaMalloc(&odl, nb * sizeof(float)));
-  CKB(cudaMalloc(&operm, nb * sizeof(int64_t)));
+  CKB(ev_alloc(ctx, &ozu, nb * sizeof(float)));
+  CKB(ev_alloc(ctx, &ozd, nb * sizeof(float)));
+  CKB(ev_alloc(ctx, &odl, nb * sizeof(float)));
+  CKB(ev_alloc(ctx, &operm, nb * sizeof(int64_t)));
   CKB(cudaMemcpyAsync(d_hist, offs.data(), n_keys * sizeof(unsigned long long),
                       cudaMemcpyHostToDevice, st));
   CKB(launch_bin_scatter(keys, n, zu, zd, dl, orig, d_hist, ozu, ozd, odl,
@@ -321,21 +321,25 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
   // column-major windows: each item's events in quads of middle-row classes
   // (k_item_order); the binned arrays are replaced by the ordered ones
   if (t.cs != 0 && !items.empty() && STRIP_ITEM_ORDER) {
+    // the boxes and keys are done with: the pool hands their memory to the
+    // ordered arrays
+    ev_free(ctx, boxes);
+    ev_free(ctx, keys);
     float *qzu = nullptr, *qzd = nullptr, *qdl = nullptr;
     int64_t* qperm = nullptr;
-    cudaError_t e = cudaMalloc(&qzu, nb * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&qzd, nb * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&qdl, nb * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&qperm, nb * sizeof(int64_t));
+    cudaError_t e = ev_alloc(ctx, &qzu, nb * sizeof(float));
+    if (e == cudaSuccess) e = ev_alloc(ctx, &qzd, nb * sizeof(float));
+    if (e == cudaSuccess) e = ev_alloc(ctx, &qdl, nb * sizeof(float));
+    if (e == cudaSuccess) e = ev_alloc(ctx, &qperm, nb * sizeof(int64_t));
     if (e == cudaSuccess)
       e = launch_item_order(ctx->s, t, d_items, (int)items.size(), ozu, ozd, odl, operm, qzu,
                             qzd, qdl, qperm, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
-      cudaFree(qzu);
-      cudaFree(qzd);
-      cudaFree(qdl);
-      cudaFree(qperm);
+      ev_free(ctx, qzu);
+      ev_free(ctx, qzd);
+      ev_free(ctx, qdl);
+      ev_free(ctx, qperm);
+      cudaStreamSynchronize(st);
       cudaFree(d_items);
       cudaFree(d_ihist);
       CKB(e);
@@ -344,10 +348,10 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
     std::swap(ozd, qzd);
     std::swap(odl, qdl);
     std::swap(operm, qperm);
-    cudaFree(qzu);
-    cudaFree(qzd);
-    cudaFree(qdl);
-    cudaFree(qperm);
+    ev_free(ctx, qzu);
+    ev_free(ctx, qzd);
+    ev_free(ctx, qdl);
+    ev_free(ctx, qperm);
   }
   cudaEventRecord(ctx->ev1, st);
   {
@@ -362,10 +366,10 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
 
   // commit
-  dfree(ctx->d_zu);
-  dfree(ctx->d_zd);
-  dfree(ctx->d_dl);
-  dfree(ctx->d_perm);
+  ev_free(ctx, ctx->d_zu);
+  ev_free(ctx, ctx->d_zd);
+  ev_free(ctx, ctx->d_dl);
+  ev_free(ctx, ctx->d_perm);
   dfree(ctx->d_items);
   dfree(ctx->d_item_hist);
   ctx->d_item_hist = d_ihist;
@@ -382,7 +386,7 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
   ctx->sub_g_begin.swap(gb);
   ctx->sub_g_count.swap(gc);
   ctx->n_binned = (int64_t)total;
-  dfree(ctx->d_wbin);  // sized for the previous binning
+  ev_free(ctx, ctx->d_wbin);  // sized for the previous binning
   ctx->n_subsets = n_subsets;
   ctx->t = t;
   ctx->max_w = wh[0];
@@ -477,10 +481,10 @@ int ensure_binning(strip_ctx* ctx, int n_subsets) {
     ctx->d_perm = pm;
     return rc;
   }
-  cudaFree(zu);
-  cudaFree(zd);
-  cudaFree(dl);
-  cudaFree(pm);
+  ev_free(ctx, zu);
+  ev_free(ctx, zd);
+  ev_free(ctx, dl);
+  ev_free(ctx, pm);
   return STRIP_OK;
 }
 
@@ -530,6 +534,22 @@ int strip_ctx_create(const strip_geometry* g, int device, strip_ctx** out) {
     ctx->sm_count = prop.multiProcessorCount;
     ctx->smem_optin = (int)prop.sharedMemPerBlockOptin;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
+    {
+      // the event buffers' pool keeps its memory between binnings (no
+      // release to the device until the context is destroyed)
+      cudaMemPoolProps props{};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.handleTypes = cudaMemHandleTypeNone;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = device;
+      if (cudaMemPoolCreate(&ctx->pool, &props) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      } else {
+        cudaGetLastError();
+        ctx->pool = nullptr;  // plain allocations
+      }
+    }
     if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
     if (cudaMalloc(&ctx->d_rho, ctx->n_pix * sizeof(float)) != cudaSuccess ||
         cudaMalloc(&ctx->d_acc_own, ctx->n_pix * sizeof(double)) != cudaSuccess ||
@@ -564,11 +584,11 @@ int strip_ctx_destroy(strip_ctx* ctx) {
   dfree(ctx->d_rho);
   dfree(ctx->d_acc_own);
   dfree(ctx->d_sens5);
-  dfree(ctx->d_wbin);
-  dfree(ctx->d_zu);
-  dfree(ctx->d_zd);
-  dfree(ctx->d_dl);
-  dfree(ctx->d_perm);
+  ev_free(ctx, ctx->d_wbin);
+  ev_free(ctx, ctx->d_zu);
+  ev_free(ctx, ctx->d_zd);
+  ev_free(ctx, ctx->d_dl);
+  ev_free(ctx, ctx->d_perm);
   dfree(ctx->d_items);
   dfree(ctx->d_item_hist);
   dfree(ctx->d_fallback);
@@ -577,7 +597,11 @@ int strip_ctx_destroy(strip_ctx* ctx) {
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   for (cudaEvent_t ev : ctx->tile_marks) cudaEventDestroy(ev);
   release_staging(ctx);
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->stream) {
+    cudaStreamSynchronize(ctx->stream);  // the pool's frees above
+    cudaStreamDestroy(ctx->stream);
+  }
+  if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   delete ctx;
   return STRIP_OK;
 }
@@ -630,14 +654,14 @@ int strip_set_events(strip_ctx* ctx, const float* zu, const float* zd,
   if (int rc = set_device(ctx)) return rc;
   float* d = nullptr;
   const size_t bytes = (size_t)std::max<int64_t>(n, 1) * sizeof(float);
-  CK(cudaMalloc(&d, 3 * bytes));
+  CK(ev_alloc(ctx, &d, 3 * bytes));
   float* dzu = d;
   float* dzd = d + std::max<int64_t>(n, 1);
   float* ddl = d + 2 * std::max<int64_t>(n, 1);
   if (n > 0) {
     const auto t0 = std::chrono::steady_clock::now();
     if (int rc = upload_soa(ctx, zu, zd, dl, n, dzu, dzd, ddl)) {
-      cudaFree(d);
+      ev_free(ctx, d);
       return rc;
     }
     ctx->stats.last_upload_ms =
@@ -645,7 +669,7 @@ int strip_set_events(strip_ctx* ctx, const float* zu, const float* zd,
   }
   ctx->n_events = n;
   int rc = bin_events(ctx, dzu, dzd, ddl, nullptr, n, n_subsets);
-  cudaFree(d);
+  ev_free(ctx, d);
   return rc;
 }
 
@@ -857,7 +881,7 @@ int adjoint_dev(strip_ctx* ctx, const double* d_w, double sz, double sdl,
   CK(cudaMemsetAsync(d_g, 0, ctx->n_pix * sizeof(double), ctx->stream));
   // the weights in binned order (read contiguously by the kernels)
   if (!ctx->d_wbin && ctx->n_binned > 0)
-    CK(cudaMalloc(&ctx->d_wbin, ctx->n_binned * sizeof(float)));
+    CK(ev_alloc(ctx, &ctx->d_wbin, ctx->n_binned * sizeof(float)));
   CK(launch_gather_weights(ctx->d_perm, d_w, ctx->n_binned, ctx->d_wbin,
                            ctx->stream));
   LaunchArgs a = base_args(ctx);
@@ -1116,6 +1140,21 @@ namespace stripmlem {
 
 int ctx_fail(strip_ctx* ctx, int code, const char* msg) {
   return fail(ctx, code, "%s", msg);
+}
+
+cudaError_t ev_alloc_bytes(strip_ctx* ctx, void** p, size_t bytes) {
+  *p = nullptr;
+  if (ctx->pool) return cudaMallocFromPoolAsync(p, std::max<size_t>(bytes, 16), ctx->pool,
+                                                ctx->stream);
+  return cudaMalloc(p, std::max<size_t>(bytes, 16));
+}
+
+void ev_free_ptr(strip_ctx* ctx, void* p) {
+  if (!p) return;
+  if (ctx->pool)
+    cudaFreeAsync(p, ctx->stream);
+  else
+    cudaFree(p);
 }
 
 int ctx_prepare_mlem(strip_ctx* ctx, int mode) {

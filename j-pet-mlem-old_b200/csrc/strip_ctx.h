@@ -13,6 +13,10 @@
 struct strip_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // stream-ordered pool of the event-sized buffers (uploads, binning
+  // scratch, binned events): it keeps freed memory for the next binning, so
+  // a new set of events costs no device allocations or unmappings
+  cudaMemPool_t pool = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   char devname[256] = {0};
   int sm_count = 148;
@@ -63,6 +67,19 @@ namespace stripmlem {
 
 // Records msg as the context's last error and returns code.
 int ctx_fail(strip_ctx* ctx, int code, const char* msg);
+// Event-sized device buffers from the context's pool (stream-ordered on the
+// context's stream; plain cudaMalloc / cudaFree without a pool).
+cudaError_t ev_alloc_bytes(strip_ctx* ctx, void** p, size_t bytes);
+void ev_free_ptr(strip_ctx* ctx, void* p);
+template <class T>
+cudaError_t ev_alloc(strip_ctx* ctx, T** p, size_t bytes) {
+  return ev_alloc_bytes(ctx, reinterpret_cast<void**>(p), bytes);
+}
+template <class T>
+void ev_free(strip_ctx* ctx, T*& p) {
+  ev_free_ptr(ctx, p);
+  p = nullptr;
+}
 // Device selected, events binned for plain MLEM (one subset), the 5-point
 // sensitivity present for STRIP_MODE_GPU.
 int ctx_prepare_mlem(strip_ctx* ctx, int mode);

@@ -1348,7 +1348,15 @@ __global__ void k_item_order(ScannerF s, Tiling t, const WorkItem* __restrict__ 
     event_setup(s, zu[i], zd[i], dl[i], e);
     return (e.tly + ((e.bry - e.tly - 1) >> 1) - wy0) & 31;
   };
-  for (int k = threadIdx.x; k < it.count; k += blockDim.x) atomicAdd(&s_n[cls(it.begin + k)], 1);
+  // class counts and, below, ranks: one shared atomic per class and warp
+  // (lanes of a class found by __match_any_sync)
+  const int lane = threadIdx.x & 31;
+  const int n_round = (it.count + blockDim.x - 1) / blockDim.x * blockDim.x;
+  for (int k = threadIdx.x; k < n_round; k += blockDim.x) {
+    const int v = k < it.count ? cls(it.begin + k) : -1;
+    const unsigned peers = __match_any_sync(kFull, v);
+    if (v >= 0 && lane == __ffs(peers) - 1) atomicAdd(&s_n[v], __popc(peers));
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     int left[32];
@@ -1379,10 +1387,16 @@ __global__ void k_item_order(ScannerF s, Tiling t, const WorkItem* __restrict__ 
     }
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < it.count; k += blockDim.x) {
+  for (int k = threadIdx.x; k < n_round; k += blockDim.x) {
     const int64_t i = it.begin + k;
-    const int v = cls(i);
-    const int r = atomicAdd(&s_cnt[v], 1);
+    const int v = k < it.count ? cls(i) : -1;
+    const unsigned peers = __match_any_sync(kFull, v);
+    const int leader = __ffs(peers) - 1;
+    int r0 = 0;
+    if (v >= 0 && lane == leader) r0 = atomicAdd(&s_cnt[v], __popc(peers));
+    r0 = __shfl_sync(kFull, r0, leader);
+    if (v < 0) continue;
+    const int r = r0 + __popc(peers & ((1u << lane) - 1u));
     const int q = s_q[v], p = s_p[v];
     const int at = r < q ? s_qbase[v] + 4 * r
                          : r < q + p ? s_pbase[v] + 2 * (r - q) : s_sbase[v] + (r - q - p);

@@ -155,7 +155,7 @@ int host_upload(strip_ctx* ctx, const void* src, size_t bytes, char* d_dst,
 int bin_triples(strip_ctx* ctx, const float* d_aos, int64_t n, int n_subsets) {
   float* d = nullptr;
   const size_t m = (size_t)std::max<int64_t>(n, 1);
-  if (cudaMalloc(&d, 3 * m * sizeof(float)) != cudaSuccess) {
+  if (ev_alloc(ctx, &d, 3 * m * sizeof(float)) != cudaSuccess) {
     cudaGetLastError();
     return upload_fail(ctx, STRIP_E_NOMEM, "no device memory for the events");
   }
@@ -167,7 +167,7 @@ int bin_triples(strip_ctx* ctx, const float* d_aos, int64_t n, int n_subsets) {
   } else {
     rc = strip_set_events_device(ctx, d, d + m, d + 2 * m, n, n_subsets);
   }
-  cudaFree(d);
+  ev_free(ctx, d);
   return rc;
 }
 
@@ -193,7 +193,7 @@ int upload_soa(strip_ctx* ctx, const float* zu, const float* zd, const float* dl
 int upload_responses(strip_ctx* ctx, const float* t, int64_t n, int n_subsets) {
   float* d_aos = nullptr;
   const size_t bytes = (size_t)n * 3 * sizeof(float);
-  if (cudaMalloc(&d_aos, std::max<size_t>(bytes, 16)) != cudaSuccess) {
+  if (ev_alloc(ctx, &d_aos, std::max<size_t>(bytes, 16)) != cudaSuccess) {
     cudaGetLastError();
     return upload_fail(ctx, STRIP_E_NOMEM, "no device memory for the events");
   }
@@ -202,7 +202,7 @@ int upload_responses(strip_ctx* ctx, const float* t, int64_t n, int n_subsets) {
   ctx->stats.last_upload_ms =
       std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (rc == STRIP_OK) rc = bin_triples(ctx, d_aos, n, n_subsets);
-  cudaFree(d_aos);
+  ev_free(ctx, d_aos);
   return rc;
 }
 
@@ -236,7 +236,7 @@ extern "C" int strip_load_responses_file(strip_ctx* ctx, const char* path,
   posix_fadvise(fd, first * 12, count * 12, POSIX_FADV_SEQUENTIAL);
   float* d_aos = nullptr;
   const size_t bytes = (size_t)count * 12;
-  if (cudaMalloc(&d_aos, std::max<size_t>(bytes, 16)) != cudaSuccess) {
+  if (ev_alloc(ctx, &d_aos, std::max<size_t>(bytes, 16)) != cudaSuccess) {
     close(fd);
     cudaGetLastError();
     return ctx_fail(ctx, STRIP_E_NOMEM, "no device memory for the events");
@@ -260,7 +260,7 @@ extern "C" int strip_load_responses_file(strip_ctx* ctx, const char* path,
   ctx->stats.last_upload_ms =
       std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (rc == STRIP_OK) rc = bin_triples(ctx, d_aos, count, n_subsets);
-  cudaFree(d_aos);
+  ev_free(ctx, d_aos);
   if (rc == STRIP_OK && n_loaded) *n_loaded = count;
   return rc;
 }
