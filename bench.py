@@ -47,9 +47,9 @@ PHANTOM = [
 SEED = 20260101
 # DRAM bytes (read + write) per event of one k_tile pass, from an ncu capture
 # of one launch over this workload's first 2e7 events (dram__bytes_read.sum
-# 244.9 MB + dram__bytes_write.sum 6.3 MB); the traffic grows with the event
+# 244.7 MB + dram__bytes_write.sum 5.1 MB); the traffic grows with the event
 # count.
-TILE_DRAM_BYTES_PER_EVENT = (244.899072e6 + 6.301696e6) / 2e7
+TILE_DRAM_BYTES_PER_EVENT = (244.702464e6 + 5.090304e6) / 2e7
 
 
 def workload_config(n_events, e2e_iters, world=1):
