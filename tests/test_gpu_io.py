@@ -87,3 +87,21 @@ def test_aos_and_pinned_setters_equal_set_events(events):
     _same(_reconstruct(set_responses), want)
     pinned = [torch.from_numpy(a).pin_memory() for a in (zu, zd, dl)]
     _same(_reconstruct(lambda r: r.set_events(*(p.numpy() for p in pinned))), want)
+
+
+def test_rebinning_one_context_equals_fresh_contexts(events):
+    """One context given event sets that shrink and grow again (its memory
+    pool hands each binning the buffers the last one freed) reconstructs as
+    a fresh context does for each set."""
+    import stripmlem as sm
+    zu, zd, dl = events
+    with sm.Reconstruction(_scanner()) as rec:
+        for n in (3_000_000, 400_000, 3_000_000, 1_300_000):
+            rec.set_events(zu[:n], zd[:n], dl[:n])
+            assert rec.stats()["n_events"] == n
+            rec.rho = np.ones((C1["n_y"], C1["n_z"]), np.float32)
+            rec(None, 2)
+            got = rec.rho.astype(np.float64)
+            want, _ = _reconstruct(lambda r: r.set_events(zu[:n], zd[:n], dl[:n]))
+            want = want.astype(np.float64)
+            assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-6, n
