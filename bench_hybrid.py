@@ -35,11 +35,11 @@ SEED = 20260202
 # 19 with its two arctangents, quotient 1), weight 2, denominator 2, scatter 2.
 FLOPS_PER_VOXEL = 63.0
 # DRAM bytes (read + write) per frame event of one k_mlem launch, from an ncu
-# capture of the first 1e6 responses of this workload (746.3 MB read + 1345.1
+# capture of the first 1e6 responses of this workload (149.6 MB read + 893.6
 # MB written, dram__bytes_read.sum / dram__bytes_write.sum of one launch): frame
 # events, LOR pixel infos and weights, and the per-warp weight slabs' lines
 # that L2 writes back before they are read again.
-MLEM_DRAM_BYTES_PER_EVENT = (746.3424e6 + 1345.082e6) / 1e6
+MLEM_DRAM_BYTES_PER_EVENT = (149.592576e6 + 893.551104e6) / 1e6
 
 
 def config(n, e2e_iters):
