@@ -459,9 +459,11 @@ def batched_throughput(local_rank, n_inst, warmup, steps, autotune=True):
                 "schedules": schedules,
                 "autotune_s": tune_s,
                 "what": "64 seeded instances (image 100-800 px per side, 1-4 mm pixels, "
-                        "1e5-2e7 events each): one MLEM step of every instance as one "
-                        "persistent tile launch + one update launch replayed from a CUDA "
-                        "graph, against strip_iterate on each context in turn"}
+                        "1e5-2e7 events each): one MLEM step of every instance -- own tile "
+                        "launches of the large instances on side streams beside a "
+                        "persistent tile launch over the small ones, one update launch -- "
+                        "replayed from a CUDA graph, against strip_iterate on each context "
+                        "in turn"}
     finally:
         for r in recs:
             r.close()

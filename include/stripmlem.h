@@ -229,9 +229,11 @@ int strip_grad_sigma_device(strip_ctx* ctx, const float* d_rho,
 /* ---- batches of reconstructions ----------------------------------------- */
 
 /* Several contexts -- each with its own geometry, events and image -- advanced
- * together: one MLEM step is one persistent launch of the tile kernel over
- * the work items of every member, the global-path launches of members with
- * oversized event boxes, and one update launch over all images; the step is
+ * together: one MLEM step is a tile launch of its own for every member with
+ * at least two work items per SM (on side streams), one persistent launch of
+ * the tile kernel over the work items of the smaller members, the global-path
+ * launches of members with oversized event boxes, and one update launch over
+ * all images; the step is
  * captured once as a CUDA graph and replayed.  The reference runs one
  * reconstruction per process; there is no counterpart.
  * Members (at most 64) share the device and the accumulation mode; their

@@ -2,11 +2,13 @@
 // strip_batch_*, strip_autotune).
 //
 // A batch advances several contexts -- each with its own geometry, events and
-// image -- together: one MLEM step is ONE persistent launch of the tile kernel
-// over the work items of every member (k_tile_batch: CTAs pull items from a
-// global counter, largest first), the global-path launches of members that
-// have overflow events, and one update launch over all images; the step is
-// captured once as a CUDA graph and replayed.  The reference runs one
+// image -- together: one MLEM step is a tile launch of its own for every
+// member with at least two work items per SM, spread over side streams, beside
+// one persistent launch per window class over the work items of the smaller
+// members (k_tile_batch: CTAs pull items from a global counter, largest
+// first), then the global-path launches of members that have overflow events
+// and one update launch over all images; the step is captured once as a CUDA
+// graph and replayed.  The reference runs one
 // reconstruction per process (reconstruction_cmd.cpp:105-301); there is no
 // batched counterpart.
 //
@@ -18,6 +20,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <new>
 #include <string>
 #include <vector>
@@ -31,6 +34,19 @@ constexpr int kNarrowSmem = kNarrowSmemBytes;
 // Work-item classes: narrow / wide windows, row-major / column-major.
 constexpr int kClasses = 4;
 inline int class_stride(int c) { return (c & 2) ? kColumnStride : 0; }
+// Members with at least this many work items per SM get a tile launch of
+// their own (k_tile, arguments in constant parameter space) instead of
+// joining the persistent launch, whose per-member arguments are indexed at
+// run time and cost registers; the own launches run on kSideStreams streams
+// forked from the batch stream, beside the persistent launches that fill
+// their tails.
+#ifndef STRIP_BATCH_SPLIT_PER_SM
+#define STRIP_BATCH_SPLIT_PER_SM 2
+#endif
+#ifndef STRIP_BATCH_STREAMS
+#define STRIP_BATCH_STREAMS 4
+#endif
+constexpr int kSideStreams = STRIP_BATCH_STREAMS;
 
 struct strip_batch {
   int device = 0;
@@ -51,7 +67,13 @@ struct strip_batch {
   int cls_begin[kClasses] = {}, cls_count[kClasses] = {}, cls_smem[kClasses] = {};
   int cls_rows[kClasses] = {};  // the most box rows of a class's events
   int* d_counter = nullptr;  // one counter per class
+  // members with a tile launch of their own, and the side stream of each
+  std::vector<int> own, own_stream;
+  int n_side = 0;
+  cudaStream_t side[kSideStreams] = {};
+  cudaEvent_t fork = nullptr, join[kSideStreams] = {};
   int64_t n_events = 0;
+  int n_work_items = 0;  // of all members, own launches included
   int launches_per_step = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -85,21 +107,36 @@ void release(strip_batch* b) {
   if (b->d_counter) cudaFree(b->d_counter);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->fork) cudaEventDestroy(b->fork);
+  for (int s = 0; s < kSideStreams; ++s) {
+    if (b->join[s]) cudaEventDestroy(b->join[s]);
+    if (b->side[s]) cudaStreamDestroy(b->side[s]);
+  }
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b->args;
   delete b;
 }
 
-// One step on the batch stream: counter reset, the persistent tile launch,
-// the members' global-path launches, the batched update.
+// One step on the batch stream: counter reset, the own tile launches of the
+// large members on the side streams beside the persistent tile launches of
+// the others, the members' global-path launches, the batched update.
 int enqueue_step(strip_batch* b) {
   BCK(cudaMemsetAsync(b->d_counter, 0, kClasses * sizeof(int), b->stream));
+  if (b->n_side > 0) {
+    BCK(cudaEventRecord(b->fork, b->stream));
+    for (int s = 0; s < b->n_side; ++s) BCK(cudaStreamWaitEvent(b->side[s], b->fork, 0));
+    for (size_t k = 0; k < b->own.size(); ++k)
+      BCK(launch_tile(OP_MLEM, b->mode, b->accum, b->args->member[b->own[k]],
+                      b->side[b->own_stream[k]]));
+    for (int s = 0; s < b->n_side; ++s) BCK(cudaEventRecord(b->join[s], b->side[s]));
+  }
   for (int c = 0; c < kClasses; ++c)
     if (b->cls_count[c] > 0)
       BCK(launch_tile_batch(b->mode, b->accum, *b->args,
                             b->d_items + b->cls_begin[c], b->cls_count[c],
                             b->d_counter + c, b->cls_smem[c], b->cls_rows[c],
                             class_stride(c), b->sm_count, b->stream));
+  for (int s = 0; s < b->n_side; ++s) BCK(cudaStreamWaitEvent(b->stream, b->join[s], 0));
   BatchUpdateArgs u{};
   u.n = (int)b->members.size();
   u.weighted = mlem_weighted(b->mode);
@@ -151,6 +188,7 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
   b->members.assign(members, members + n_members);
   int rc = STRIP_OK;
   std::vector<BatchItem> items;
+  std::vector<std::pair<int, int>> own;  // (work items, member)
   for (int m = 0; m < n_members && rc == STRIP_OK; ++m) {
     strip_ctx* c = members[m];
     rc = ctx_prepare_mlem(c, mode);
@@ -163,6 +201,13 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
     b->cls_smem[cls] = std::max(b->cls_smem[cls], c->t.smem_bytes);
     b->cls_rows[cls] = std::max(b->cls_rows[cls], c->t.max_rows);
     b->n_events += c->n_events;
+    b->n_work_items += b->args->member[m].n_items;
+    if (b->args->member[m].n_items > 0 &&
+        b->args->member[m].n_items >= STRIP_BATCH_SPLIT_PER_SM * b->sm_count) {
+      own.emplace_back(b->args->member[m].n_items, m);
+      b->launches_per_step += 1 + (b->args->member[m].g_count > 0);
+      continue;
+    }
     for (int i = 0; i < b->args->member[m].n_items; ++i) {
       const WorkItem& w = c->items[i];
       items.push_back(BatchItem{m, w.tile, w.count, cls, w.begin, i, 0});
@@ -181,13 +226,30 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
     for (int c = 1; c < kClasses; ++c) b->cls_begin[c] = b->cls_begin[c - 1] + b->cls_count[c - 1];
     b->launches_per_step += 1;
     for (int c = 0; c < kClasses; ++c) b->launches_per_step += b->cls_count[c] > 0;
+    // own launches, largest first, each on the side stream with the fewest
+    // work items so far
+    std::sort(own.begin(), own.end(), std::greater<std::pair<int, int>>());
+    int64_t load[kSideStreams] = {};
+    b->n_side = std::min<int>(kSideStreams, (int)own.size());
+    for (const auto& o : own) {
+      const int s = (int)(std::min_element(load, load + b->n_side) - load);
+      load[s] += o.first;
+      b->own.push_back(o.second);
+      b->own_stream.push_back(s);
+    }
     do {
       if (cudaSetDevice(b->device) != cudaSuccess) { rc = STRIP_E_CUDA; break; }
       if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-          cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
+          cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+          cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) {
         rc = STRIP_E_CUDA;
         break;
       }
+      for (int s = 0; s < b->n_side && rc == STRIP_OK; ++s)
+        if (cudaStreamCreateWithFlags(&b->side[s], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b->join[s], cudaEventDisableTiming) != cudaSuccess)
+          rc = STRIP_E_CUDA;
+      if (rc != STRIP_OK) break;
       if (cudaMalloc(&b->d_items, std::max<size_t>(items.size(), 1) * sizeof(BatchItem)) != cudaSuccess ||
           cudaMalloc(&b->d_counter, kClasses * sizeof(int)) != cudaSuccess) {
         rc = STRIP_E_NOMEM;
@@ -257,7 +319,7 @@ int strip_batch_stats(strip_batch* b, double* last_iterate_ms, int64_t* n_events
   if (!b) return STRIP_E_INVALID;
   if (last_iterate_ms) *last_iterate_ms = b->last_ms;
   if (n_events) *n_events = b->n_events;
-  if (n_work_items) *n_work_items = b->n_items;
+  if (n_work_items) *n_work_items = b->n_work_items;
   if (launches_per_iteration) *launches_per_iteration = b->launches_per_step;
   return STRIP_OK;
 }
