@@ -1,6 +1,7 @@
-"""Batches of reconstructions (one persistent tile launch per step, CUDA graph
-replay) and the schedule autotuner, against single-context runs and the FP64
-oracle."""
+"""Batches of reconstructions (per step: own tile launches of the members with
+at least two work items per SM, one persistent tile launch over the others'
+items, CUDA graph replay) and the schedule autotuner, against single-context
+runs and the FP64 oracle."""
 import numpy as np
 import pytest
 
@@ -56,6 +57,42 @@ def test_batch_equals_single_contexts(members, mode):
         assert st["n_events"] == sum(len(ev[0]) for _, _, ev in members)
         assert st["launches_per_iteration"] >= 2
         assert st["last_iterate_ms"] > 0
+        for rec, single, (sc, g, ev) in zip(recs, singles, members):
+            img = rec.rho
+            assert rel(img, single) < 2e-5
+            ref = orc.mlem_f64(g, *ev, 3, mode=mode, sets_f32=True)
+            assert rel(img, ref) < 1e-4
+    finally:
+        for r in recs:
+            r.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_batch_own_launches_equal_single_contexts(members, mode):
+    """Members 0 and 1 binned in 64-event work items (940 and 625 items, past
+    two per SM) take tile launches of their own on the side streams; members
+    2 and 3 stay in the persistent launch."""
+    import stripmlem as sm
+    item_events = [64, 64, 0, 0]
+    singles, recs = [], []
+    try:
+        for (sc, g, ev), k in zip(members, item_events):
+            with sm.Reconstruction(sc, mode=mode) as r:
+                r.set_item_events(k)
+                r.set_events(*ev)
+                r(None, 3)
+                singles.append(r.rho)
+            rec = sm.Reconstruction(sc, mode=mode)
+            rec.set_item_events(k)
+            rec.set_events(*ev)
+            recs.append(rec)
+        items = [r.stats()["n_work_items"] for r in recs]
+        assert min(items[:2]) >= 2 * 148 and max(items[2:]) < 2 * 148
+        with sm.Batch(recs, mode=mode) as batch:
+            batch(3)
+            st = batch.stats()
+        assert st["n_work_items"] == sum(items)
+        assert st["launches_per_iteration"] >= 4  # 2 own + persistent + update
         for rec, single, (sc, g, ev) in zip(recs, singles, members):
             img = rec.rho
             assert rel(img, single) < 2e-5
