@@ -339,8 +339,10 @@ class Reconstruction:
 
 class Batch:
     """Several Reconstructions (each with its own geometry, events and
-    image) advanced together: one persistent tile launch and one update
-    launch per MLEM step, replayed from a CUDA graph (strip_batch_*).
+    image) advanced together: per MLEM step, a tile launch of its own for
+    every member with at least two work items per SM (on side streams), one
+    persistent tile launch over the others' items and one update launch,
+    replayed from a CUDA graph (strip_batch_*).
     Re-create the batch after set_events on a member."""
 
     def __init__(self, reconstructions, mode=MODE_CPU):
