@@ -274,7 +274,8 @@ int strip_autotune(strip_ctx* ctx, int mode, strip_tuning* best);
 int strip_set_schedule(strip_ctx* ctx, int tile, int grab);
 /* Largest tile work item, in events (1..8000); 0 (the default) picks it per
  * binning: enough items for about eight waves of the device, at least 2048
- * and at most 8000 events.  Re-bins the events when the context has some.
+ * and at most 8000 events, the last wave's worth of each subset's items cut
+ * into quarter pieces.  Re-bins the events when the context has some.
  * The item size changes the work decomposition and the fixed-point scale of
  * each item's window, not the result beyond rounding; a small event set
  * binned with 8000-event items runs the arithmetic of a large one. */

@@ -112,6 +112,17 @@ KernelF make_kernel(double sigma_z, double sigma_dl, float pw) {
 #ifndef STRIP_ITEM_ORDER
 #define STRIP_ITEM_ORDER 1
 #endif
+// With the item size chosen per binning, the last STRIP_TAIL_WAVES waves of
+// a subset's work items (by events, one wave = two CTAs per SM, each with a
+// full item) are cut into STRIP_TAIL_PIECES pieces each, so the launch's last
+// CTAs finish close together without the per-item cost of small items
+// everywhere (0: off).
+#ifndef STRIP_TAIL_PIECES
+#define STRIP_TAIL_PIECES 4
+#endif
+#ifndef STRIP_TAIL_WAVES
+#define STRIP_TAIL_WAVES 1
+#endif
 
 namespace {
 
@@ -289,6 +300,30 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
         any = true;
       }
       if (!any) break;
+    }
+    if (STRIP_TAIL_PIECES > 1 && ctx->item_events <= 0) {
+      // the subset's last items, back to about one wave's worth of events
+      // (an item size set by hand is kept as set)
+      const int64_t tail = (int64_t)STRIP_TAIL_WAVES * ctx->sm_count * 2 * chunk;
+      size_t k = items.size();
+      int64_t acc = 0;
+      while (k > (size_t)ib[sb] && acc + items[k - 1].count <= tail) acc += items[--k].count;
+      if (k < items.size()) {
+        // piece p of every item before piece p + 1 of any: the CTAs resident
+        // at one time still work on different tiles
+        std::vector<WorkItem> cut;
+        for (int pc = 0; pc < STRIP_TAIL_PIECES; ++pc)
+          for (size_t i = k; i < items.size(); ++i) {
+            const WorkItem w = items[i];
+            const int64_t piece = (w.count + STRIP_TAIL_PIECES - 1) / STRIP_TAIL_PIECES;
+            const int64_t o = pc * piece;
+            if (o < w.count)
+              cut.push_back(WorkItem{w.tile, (int32_t)std::min<int64_t>(piece, w.count - o),
+                                     w.begin + o});
+          }
+        items.resize(k);
+        items.insert(items.end(), cut.begin(), cut.end());
+      }
     }
     ic[sb] = (int)items.size() - ib[sb];
     const int gkey = sb * (t.n_tiles + 1) + t.n_tiles;
