@@ -237,7 +237,8 @@ int strip_grad_sigma_device(strip_ctx* ctx, const float* d_rho,
  * captured once as a CUDA graph and replayed.  The reference runs one
  * reconstruction per process; there is no counterpart.
  * Members (at most 64) share the device and the accumulation mode; their
- * events are re-binned for plain MLEM (one subset).  A batch holds the
+ * events are re-binned for plain MLEM (one subset), without the last wave
+ * of work items cut into pieces.  A batch holds the
  * members' buffers as they were at creation: re-create it after
  * strip_set_events, strip_set_accumulator or a re-binning of a member
  * (strip_set_image keeps the buffers).  While a batch iterates its members

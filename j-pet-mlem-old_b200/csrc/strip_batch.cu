@@ -46,6 +46,12 @@ inline int class_stride(int c) { return (c & 2) ? kColumnStride : 0; }
 #ifndef STRIP_BATCH_STREAMS
 #define STRIP_BATCH_STREAMS 4
 #endif
+// Members are binned without the cut last wave: the persistent CTAs balance
+// the small members' items, and the side streams overlap the own launches'
+// tails (measured on 64 instances: 984 Mevent*iter/s unsplit, 938 split).
+#ifndef STRIP_BATCH_UNSPLIT
+#define STRIP_BATCH_UNSPLIT 1
+#endif
 constexpr int kSideStreams = STRIP_BATCH_STREAMS;
 
 struct strip_batch {
@@ -196,14 +202,23 @@ int strip_batch_create(strip_ctx* const* members, int n_members, int mode,
       b->err = "member " + std::to_string(m) + ": " + c->err;
       break;
     }
+    if (STRIP_BATCH_UNSPLIT && c->tail_split) {
+      c->tail_split = false;
+      rc = ctx_rebin(c, c->tile_pref);
+      if (rc != STRIP_OK) {
+        b->err = "member " + std::to_string(m) + ": " + c->err;
+        break;
+      }
+    }
     b->args->member[m] = ctx_mlem_args(c, mode);
+    const bool own_launch =
+        b->args->member[m].n_items >= STRIP_BATCH_SPLIT_PER_SM * b->sm_count;
     const int cls = (c->t.smem_bytes > kNarrowSmem) + (c->t.cs != 0 ? 2 : 0);
     b->cls_smem[cls] = std::max(b->cls_smem[cls], c->t.smem_bytes);
     b->cls_rows[cls] = std::max(b->cls_rows[cls], c->t.max_rows);
     b->n_events += c->n_events;
     b->n_work_items += b->args->member[m].n_items;
-    if (b->args->member[m].n_items > 0 &&
-        b->args->member[m].n_items >= STRIP_BATCH_SPLIT_PER_SM * b->sm_count) {
+    if (own_launch && b->args->member[m].n_items > 0) {
       own.emplace_back(b->args->member[m].n_items, m);
       b->launches_per_step += 1 + (b->args->member[m].g_count > 0);
       continue;

@@ -301,7 +301,7 @@ int bin_events(strip_ctx* ctx, const float* zu, const float* zd,
       }
       if (!any) break;
     }
-    if (STRIP_TAIL_PIECES > 1 && ctx->item_events <= 0) {
+    if (STRIP_TAIL_PIECES > 1 && ctx->item_events <= 0 && ctx->tail_split) {
       // the subset's last items, back to about one wave's worth of events
       // (an item size set by hand is kept as set)
       const int64_t tail = (int64_t)STRIP_TAIL_WAVES * ctx->sm_count * 2 * chunk;

@@ -32,6 +32,7 @@ struct strip_ctx {
   int tile_pref = 32;  // tile edge in pixels (autotuned or 32)
   int grab = 32;       // events a warp takes per counter step (autotuned or 32)
   int item_events = 0;  // largest work item in events (0: chosen per binning)
+  bool tail_split = true;  // cut the last wave of items into pieces (binning)
   float* d_sens5 = nullptr;
   float* d_wbin = nullptr;  // adjoint weights in binned order (n_binned, binary32)
   // binned events

@@ -70,8 +70,9 @@ def test_batch_equals_single_contexts(members, mode):
 @pytest.mark.parametrize("mode", [0, 1])
 def test_batch_own_launches_equal_single_contexts(members, mode):
     """Members 0 and 1 binned in 64-event work items (940 and 625 items, past
-    two per SM) take tile launches of their own on the side streams; members
-    2 and 3 stay in the persistent launch."""
+    two per SM) take tile launches of their own on the side
+    streams; members 2 and 3 stay in the persistent launch (all re-binned
+    without the cut last wave)."""
     import stripmlem as sm
     item_events = [64, 64, 0, 0]
     singles, recs = [], []
@@ -86,11 +87,11 @@ def test_batch_own_launches_equal_single_contexts(members, mode):
             rec.set_item_events(k)
             rec.set_events(*ev)
             recs.append(rec)
-        items = [r.stats()["n_work_items"] for r in recs]
-        assert min(items[:2]) >= 2 * 148 and max(items[2:]) < 2 * 148
         with sm.Batch(recs, mode=mode) as batch:
             batch(3)
             st = batch.stats()
+            items = [r.stats()["n_work_items"] for r in recs]
+        assert min(items[:2]) >= 2 * 148 and max(items[2:]) < 2 * 148
         assert st["n_work_items"] == sum(items)
         assert st["launches_per_iteration"] >= 4  # 2 own + persistent + update
         for rec, single, (sc, g, ev) in zip(recs, singles, members):
